@@ -1,0 +1,102 @@
+"""ctypes binding of libdimspers_b200.so (the C ABI in include/dimspers_b200.h).
+
+The library is built in-tree (``python -m dimspers_b200.build``).  There is
+no CPU fallback: if the shared library is missing, importing the solver API
+raises immediately.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdimspers_b200.so")
+
+DP_OK, DP_NOT_CONVERGED, DP_BREAKDOWN, DP_BAD_ARG, DP_CUDA_ERROR, DP_DEVICE_TIMEOUT = range(6)
+DP_PRESSURE_CONTINUOUS, DP_PRESSURE_DISCONTINUOUS = 0, 1
+DP_PREC_FP64, DP_PREC_FP32_REFINED = 0, 1
+DP_MEM_HOST, DP_MEM_DEVICE = 0, 1
+DP_INNER_MG, DP_INNER_JACOBI = 0, 1
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("nr_cells", C.c_int32), ("ntheta_cells", C.c_int32), ("r_in", C.c_double),
+                ("r_out", C.c_double), ("pressure_space", C.c_int32), ("device", C.c_int32),
+                ("pin_rotation", C.c_int32)]
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("rtol", C.c_double), ("itmax", C.c_int32), ("itmin", C.c_int32),
+                ("precision", C.c_int32), ("inner_pc", C.c_int32), ("inner_rtol", C.c_double),
+                ("inner_itmax", C.c_int32), ("remove_rotation", C.c_int32), ("use_guess", C.c_int32),
+                ("verbose", C.c_int32), ("cheb_degree", C.c_int32), ("inner_rtol32", C.c_double),
+                ("max_refine", C.c_int32)]
+
+
+class SolveReport(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("inner_iterations", C.c_int64),
+                ("relres", C.c_double), ("r0", C.c_double), ("omega", C.c_double),
+                ("div_residual", C.c_double), ("mom_residual", C.c_double),
+                ("t_assemble_ms", C.c_double), ("t_setup_ms", C.c_double), ("t_solve_ms", C.c_double),
+                ("fallback_used", C.c_int32), ("mg_levels", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_I64 = C.POINTER(C.c_int64)
+_I32 = C.POINTER(C.c_int32)
+
+# name -> (restype, argtypes); every entry of include/dimspers_b200.h
+SIGNATURES = {
+    "dp_mesh_sizes": (C.c_int, [C.POINTER(MeshDesc), _I64, _I64, _I64, _I64]),
+    "dp_mesh_build": (C.c_int, [C.POINTER(MeshDesc), _I64, _D, _D, _I32, _I32]),
+    "dp_mesh_free_slip": (C.c_int, [C.POINTER(MeshDesc), _I64, _I64]),
+    "dp_status_string": (C.c_char_p, [C.c_int]),
+    "dp_ctx_create": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(_P)]),
+    "dp_ctx_destroy": (None, [_P]),
+    "dp_last_error": (C.c_char_p, [_P]),
+    "dp_ctx_stream": (_P, [_P]),
+    "dp_get_connectivity": (C.c_int, [_P, _I64, _I32]),
+    "dp_set_material": (C.c_int, [_P, _P, C.c_int64, C.POINTER(_P), C.c_int64, _P, C.c_double, C.c_int32]),
+    "dp_set_material_ti": (C.c_int, [_P, _P, C.c_int64, _P, _P, _P, _P, C.c_double, C.c_int32]),
+    "dp_fse_director": (C.c_int, [_P, _P, _P, _P, C.c_int32]),
+    "dp_assemble": (C.c_int, [_P, C.c_int32]),
+    "dp_get_element_matrices": (C.c_int, [_P, _P, _P, _P, _P]),
+    "dp_solve": (C.c_int, [_P, _P, _P, _P, C.POINTER(SolveOpts), C.POINTER(SolveReport), C.c_int32]),
+    "dp_apply_K": (C.c_int, [_P, _P, _P, C.c_int32]),
+    "dp_apply_G": (C.c_int, [_P, _P, _P, C.c_int32]),
+    "dp_apply_GT": (C.c_int, [_P, _P, _P, C.c_int32]),
+    "dp_get_rhs": (C.c_int, [_P, _P, _P]),
+    "dp_default_opts": (None, [C.POINTER(SolveOpts)]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load (once) and return the shared library; raises if it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m dimspers_b200.build` "
+                               "(the Stokes path has no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+class DPError(RuntimeError):
+    def __init__(self, status, msg):
+        self.status = status
+        super().__init__(f"{lib().dp_status_string(status).decode()}: {msg}")
+
+
+def check(status, ctx=None):
+    if status != DP_OK:
+        msg = lib().dp_last_error(ctx).decode(errors="replace")
+        raise DPError(status, msg)

@@ -1,0 +1,523 @@
+// C ABI entry points (include/dimspers_b200.h).  Every entry point catches
+// CUDA and host errors and turns them into a status code plus a message that
+// dp_last_error() returns; nothing here exits or aborts.
+#include <chrono>
+#include <cstring>
+#include <exception>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/dimspers_b200.h"
+#include "kernels.cuh"
+#include "mg.cuh"
+#include "solver.cuh"
+
+struct dp_ctx {
+  dp::Ctx c;
+};
+
+namespace dp {
+
+static thread_local std::string g_err;
+
+Ctx::~Ctx() {
+  mg_free(*this);
+  cudaFree(theta_lat); cudaFree(r_lat); cudaFree(ref2lat);
+  cudaFree(eta); cudaFree(C); cudaFree(rho_lat); cudaFree(rho_ref);
+  cudaFree(K64); cudaFree(K32); cudaFree(Gp); cudaFree(F); cudaFree(pc); cudaFree(Fscale);
+  cudaFree(scal); cudaFreeHost(h_scal); cudaFree(partial); cudaFree(counter);
+  for (void* p : work) cudaFree(p);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+struct BadArg : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+template <typename F>
+static int guarded(Ctx* c, F&& f) {
+  try {
+    return f();
+  } catch (const CudaError& e) {
+    std::string m = std::string("CUDA error ") + cudaGetErrorName(e.e) + " (" + cudaGetErrorString(e.e) + ") in " +
+                    e.what + " line " + std::to_string(e.line);
+    if (c) c->err = m; else g_err = m;
+    return DP_CUDA_ERROR;
+  } catch (const BadArg& e) {
+    if (c) c->err = e.what(); else g_err = e.what();
+    return DP_BAD_ARG;
+  } catch (const std::exception& e) {
+    if (c) c->err = e.what(); else g_err = e.what();
+    return DP_BAD_ARG;
+  }
+}
+
+static void check(const dp_mesh_desc* d) {
+  if (!d) throw BadArg("null mesh description");
+  const std::string m = check_desc(d->nr_cells, d->ntheta_cells, d->r_in, d->r_out, d->pressure_space);
+  if (!m.empty()) throw BadArg(m);
+}
+
+static cudaMemcpyKind kind_in(int mem) { return mem == DP_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice; }
+static cudaMemcpyKind kind_out(int mem) { return mem == DP_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost; }
+
+template <typename T>
+static void dalloc(T** p, size_t n) {
+  DP_CUDA(cudaMalloc((void**)p, sizeof(T) * (n ? n : 1)));
+}
+
+static void upload_eta(Ctx& c, const double* eta_ip, int64_t ld, int mem) {
+  const int64_t nel = c.fine.nel;
+  if (!eta_ip) throw BadArg("eta_ip is null");
+  if (ld < nel) throw BadArg("ld_eta < nel");
+  for (int ip = 0; ip < kNip; ++ip)
+    DP_CUDA(cudaMemcpyAsync(c.eta + ip * nel, eta_ip + ip * ld, sizeof(double) * nel, kind_in(mem), c.stream));
+}
+
+static void upload_rho(Ctx& c, const double* rho, double g, int mem) {
+  if (!rho) throw BadArg("rho_node is null");
+  DP_CUDA(cudaMemcpyAsync(c.rho_ref, rho, sizeof(double) * c.fine.nnod, kind_in(mem), c.stream));
+  launch_gather_ref2lat(c, c.rho_ref, c.rho_lat, 1);
+  c.g = g;
+}
+
+static void ensure_C(Ctx& c, int64_t n) {
+  static_cast<void>(n);
+  if (!c.C) dalloc(&c.C, 36 * c.fine.nel);
+}
+
+static SolveCfg make_cfg(const dp_solve_opts* o) {
+  SolveCfg cfg;
+  dp_solve_opts d;
+  dp_default_opts(&d);
+  if (!o) o = &d;
+  cfg.rtol = o->rtol;
+  cfg.itmax = o->itmax;
+  cfg.itmin = o->itmin;
+  cfg.precision = o->precision;
+  cfg.inner_pc = o->inner_pc;
+  cfg.inner_rtol = o->inner_rtol;
+  cfg.inner_itmax = o->inner_itmax;
+  cfg.remove_rotation = o->remove_rotation;
+  cfg.use_guess = o->use_guess;
+  cfg.verbose = o->verbose;
+  if (o->cheb_degree > 0) cfg.mg.cheb_degree = o->cheb_degree;
+  if (o->inner_rtol32 > 0) cfg.inner_rtol32 = o->inner_rtol32;
+  if (o->max_refine > 0) cfg.max_refine = o->max_refine;
+  if (!(cfg.rtol > 0) || cfg.itmax < 1 || cfg.itmin < 0 || !(cfg.inner_rtol > 0) || cfg.inner_itmax < 1)
+    throw BadArg("invalid solve options");
+  if (cfg.precision != 0 && cfg.precision != 1) throw BadArg("precision must be 0 or 1");
+  if (cfg.inner_pc != 0 && cfg.inner_pc != 1) throw BadArg("inner_pc must be 0 or 1");
+  return cfg;
+}
+
+__global__ void k_f64_to_f32(const double* a, float* b, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+
+}  // namespace dp
+
+using namespace dp;
+
+extern "C" {
+
+void dp_default_opts(dp_solve_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->rtol = 1e-8;
+  o->itmax = 200;
+  o->itmin = 10;
+  o->precision = DP_PREC_FP64;
+  o->inner_pc = DP_INNER_MG;
+  o->inner_rtol = 1e-10;
+  o->inner_itmax = 500;
+  o->remove_rotation = 1;
+  o->use_guess = 0;
+  o->verbose = 0;
+  o->cheb_degree = 3;
+  o->inner_rtol32 = 1e-5;
+  o->max_refine = 6;
+}
+
+const char* dp_status_string(int s) {
+  switch (s) {
+    case DP_OK: return "OK";
+    case DP_NOT_CONVERGED: return "NOT_CONVERGED";
+    case DP_BREAKDOWN: return "BREAKDOWN";
+    case DP_BAD_ARG: return "BAD_ARG";
+    case DP_CUDA_ERROR: return "CUDA_ERROR";
+    case DP_DEVICE_TIMEOUT: return "DEVICE_TIMEOUT";
+    default: return "UNKNOWN";
+  }
+}
+
+int dp_mesh_sizes(const dp_mesh_desc* d, int64_t* nel, int64_t* nnod, int64_t* npres, int64_t* nfixed) {
+  return guarded(nullptr, [&] {
+    check(d);
+    mesh_sizes(d->nr_cells, d->ntheta_cells, d->pressure_space, nel, nnod, npres, nfixed);
+    if (nfixed && d->pin_rotation) *nfixed += 1;
+    return (int)DP_OK;
+  });
+}
+
+int dp_mesh_build(const dp_mesh_desc* d, int64_t* e2n, double* theta, double* r, int32_t* colors, int32_t* ncolors) {
+  return guarded(nullptr, [&] {
+    check(d);
+    Mesh m;
+    build_mesh(m, d->nr_cells, d->ntheta_cells, d->r_in, d->r_out, d->pressure_space, colors || ncolors);
+    if (e2n)
+      for (int64_t i = 0; i < 6 * m.nel; ++i) e2n[i] = m.e2n[i] + 1;
+    if (theta) std::memcpy(theta, m.theta.data(), sizeof(double) * m.nnod);
+    if (r) std::memcpy(r, m.r.data(), sizeof(double) * m.nnod);
+    if (colors) std::memcpy(colors, m.colors.data(), sizeof(int32_t) * m.nel);
+    if (ncolors) *ncolors = m.ncolors;
+    return (int)DP_OK;
+  });
+}
+
+int dp_mesh_free_slip(const dp_mesh_desc* d, int64_t* omega, int64_t* nomega) {
+  return guarded(nullptr, [&] {
+    check(d);
+    Mesh m;
+    build_mesh(m, d->nr_cells, d->ntheta_cells, d->r_in, d->r_out, d->pressure_space, false);
+    std::vector<int64_t> om = m.omega;
+    if (d->pin_rotation) om.push_back(2 * (int64_t)d->nr_cells);  // u_theta of node nr (0-based 2*(nr-1))
+    if (nomega) *nomega = (int64_t)om.size();
+    if (omega)
+      for (size_t i = 0; i < om.size(); ++i) omega[i] = om[i] + 1;
+    return (int)DP_OK;
+  });
+}
+
+int dp_ctx_create(const dp_mesh_desc* d, dp_ctx** out) {
+  if (!out) return DP_BAD_ARG;
+  *out = nullptr;
+  dp_ctx* h = nullptr;
+  int st = guarded(nullptr, [&] {
+    check(d);
+    int ndev = 0;
+    DP_CUDA(cudaGetDeviceCount(&ndev));
+    if (d->device < 0 || d->device >= ndev) throw BadArg("device ordinal out of range");
+    const int64_t nel = 2 * (int64_t)d->nr_cells * d->ntheta_cells;
+    if (nel * kKe >= ((int64_t)1 << 31)) throw BadArg("mesh too large for 32-bit element indexing");
+    h = new dp_ctx();
+    Ctx& c = h->c;
+    c.device = d->device;
+    DP_CUDA(cudaSetDevice(c.device));
+    build_mesh(c.mesh, d->nr_cells, d->ntheta_cells, d->r_in, d->r_out, d->pressure_space, true);
+    c.fine.ncr = d->nr_cells;
+    c.fine.nct = d->ntheta_cells;
+    c.fine.pin = d->pin_rotation ? 1 : 0;
+    c.fine.nel = c.mesh.nel;
+    c.fine.nnod = c.mesh.nnod;
+    DP_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    upload_quadrature_constants();
+    upload_mg_constants();
+    const int64_t nn = c.mesh.nnod, np = c.mesh.npres;
+    std::vector<double> tl(nn), rl(nn);
+    for (int64_t i = 0; i < nn; ++i) {
+      tl[c.mesh.ref2lat[i]] = c.mesh.theta[i];
+      rl[c.mesh.ref2lat[i]] = c.mesh.r[i];
+    }
+    dalloc(&c.theta_lat, nn);
+    dalloc(&c.r_lat, nn);
+    dalloc(&c.ref2lat, nn);
+    DP_CUDA(cudaMemcpy(c.theta_lat, tl.data(), sizeof(double) * nn, cudaMemcpyHostToDevice));
+    DP_CUDA(cudaMemcpy(c.r_lat, rl.data(), sizeof(double) * nn, cudaMemcpyHostToDevice));
+    DP_CUDA(cudaMemcpy(c.ref2lat, c.mesh.ref2lat.data(), sizeof(int64_t) * nn, cudaMemcpyHostToDevice));
+    dalloc(&c.eta, kNip * nel);
+    dalloc(&c.rho_lat, nn);
+    dalloc(&c.rho_ref, nn);
+    dalloc(&c.K64, kKe * nel);
+    dalloc(&c.Gp, kGe * nel);
+    dalloc(&c.F, 2 * nn);
+    dalloc(&c.pc, np);
+    dalloc(&c.scal, 64);
+    DP_CUDA(cudaMemset(c.scal, 0, sizeof(double) * 64));
+    DP_CUDA(cudaMallocHost((void**)&c.h_scal, sizeof(double) * 64));
+    dalloc(&c.partial, 4 * 1024);
+    dalloc(&c.counter, 1);
+    DP_CUDA(cudaMemset(c.counter, 0, sizeof(unsigned int)));
+    c.work.assign(W_COUNT, nullptr);
+    for (int w = 0; w < W_COUNT; ++w) {
+      size_t bytes;
+      if (w <= W_SQ) bytes = sizeof(double) * np;
+      else if (w <= W_RES) bytes = sizeof(double) * 2 * nn;
+      else if (w <= W_F_AP) bytes = sizeof(float) * 2 * nn;
+      else if (w == W_P) bytes = sizeof(double) * np;
+      else bytes = sizeof(double) * 2 * nn;
+      DP_CUDA(cudaMalloc(&c.work[w], bytes ? bytes : 8));
+    }
+    return (int)DP_OK;
+  });
+  if (st != DP_OK) {
+    delete h;
+    return st;
+  }
+  *out = h;
+  return DP_OK;
+}
+
+void dp_ctx_destroy(dp_ctx* h) {
+  if (!h) return;
+  cudaSetDevice(h->c.device);
+  if (h->c.stream) cudaStreamSynchronize(h->c.stream);
+  delete h;
+}
+
+const char* dp_last_error(const dp_ctx* h) { return h ? h->c.err.c_str() : g_err.c_str(); }
+
+void* dp_ctx_stream(dp_ctx* h) { return h ? (void*)h->c.stream : nullptr; }
+
+int dp_get_connectivity(dp_ctx* h, int64_t* e2n, int32_t* colors) {
+  if (!h) return DP_BAD_ARG;
+  Ctx& c = h->c;
+  return guarded(&c, [&] {
+    if (e2n)
+      for (int64_t i = 0; i < 6 * c.mesh.nel; ++i) e2n[i] = c.mesh.e2n[i] + 1;
+    if (colors) std::memcpy(colors, c.mesh.colors.data(), sizeof(int32_t) * c.mesh.nel);
+    return (int)DP_OK;
+  });
+}
+
+int dp_set_material(dp_ctx* h, const double* eta_ip, int64_t ld_eta, const double* const* C6, int64_t ld_C,
+                    const double* rho_node, double g, int32_t mem) {
+  if (!h) return DP_BAD_ARG;
+  Ctx& c = h->c;
+  return guarded(&c, [&] {
+    DP_CUDA(cudaSetDevice(c.device));
+    upload_eta(c, eta_ip, ld_eta, mem);
+    if (C6) {
+      const int64_t nel = c.fine.nel;
+      if (ld_C < nel) throw BadArg("ld_C < nel");
+      ensure_C(c, 36 * nel);
+      for (int f = 0; f < 6; ++f) {
+        if (!C6[f]) throw BadArg("null tensor field");
+        for (int ip = 0; ip < kNip; ++ip)
+          DP_CUDA(cudaMemcpyAsync(c.C + ((size_t)f * 6 + ip) * nel, C6[f] + ip * ld_C, sizeof(double) * nel,
+                                  kind_in(mem), c.stream));
+      }
+      c.mat_kind = MAT_FULL;
+    } else {
+      c.mat_kind = MAT_ISO;
+    }
+    upload_rho(c, rho_node, g, mem);
+    c.assembled = -1;
+    DP_CUDA(cudaStreamSynchronize(c.stream));
+    return (int)DP_OK;
+  });
+}
+
+int dp_set_material_ti(dp_ctx* h, const double* eta_ip, int64_t ld_eta, const double* delta, const double* dir_x,
+                       const double* dir_y, const double* rho_node, double g, int32_t mem) {
+  if (!h) return DP_BAD_ARG;
+  Ctx& c = h->c;
+  return guarded(&c, [&] {
+    DP_CUDA(cudaSetDevice(c.device));
+    if (!delta || !dir_x || !dir_y) throw BadArg("null delta / director");
+    upload_eta(c, eta_ip, ld_eta, mem);
+    const int64_t nel = c.fine.nel;
+    ensure_C(c, 3 * nel);
+    DP_CUDA(cudaMemcpyAsync(c.C, delta, sizeof(double) * nel, kind_in(mem), c.stream));
+    DP_CUDA(cudaMemcpyAsync(c.C + nel, dir_x, sizeof(double) * nel, kind_in(mem), c.stream));
+    DP_CUDA(cudaMemcpyAsync(c.C + 2 * nel, dir_y, sizeof(double) * nel, kind_in(mem), c.stream));
+    c.mat_kind = MAT_TI;
+    upload_rho(c, rho_node, g, mem);
+    c.assembled = -1;
+    DP_CUDA(cudaStreamSynchronize(c.stream));
+    return (int)DP_OK;
+  });
+}
+
+int dp_fse_director(dp_ctx* h, const double* F, double* dir_x, double* dir_y, int32_t mem) {
+  if (!h) return DP_BAD_ARG;
+  Ctx& c = h->c;
+  return guarded(&c, [&] {
+    DP_CUDA(cudaSetDevice(c.device));
+    if (!F || !dir_x || !dir_y) throw BadArg("null argument");
+    const int64_t nel = c.fine.nel;
+    double *dF = nullptr, *dx = nullptr, *dy = nullptr;
+    const bool host = mem != DP_MEM_DEVICE;
+    if (host) {
+      dalloc(&dF, 4 * nel);
+      dalloc(&dx, nel);
+      dalloc(&dy, nel);
+      DP_CUDA(cudaMemcpyAsync(dF, F, sizeof(double) * 4 * nel, cudaMemcpyHostToDevice, c.stream));
+    }
+    launch_fse_director(c, host ? dF : F, host ? dx : dir_x, host ? dy : dir_y, nel);
+    if (host) {
+      DP_CUDA(cudaMemcpyAsync(dir_x, dx, sizeof(double) * nel, cudaMemcpyDeviceToHost, c.stream));
+      DP_CUDA(cudaMemcpyAsync(dir_y, dy, sizeof(double) * nel, cudaMemcpyDeviceToHost, c.stream));
+    }
+    DP_CUDA(cudaStreamSynchronize(c.stream));
+    cudaFree(dF); cudaFree(dx); cudaFree(dy);
+    return (int)DP_OK;
+  });
+}
+
+int dp_assemble(dp_ctx* h, int32_t precision) {
+  if (!h) return DP_BAD_ARG;
+  Ctx& c = h->c;
+  return guarded(&c, [&] {
+    DP_CUDA(cudaSetDevice(c.device));
+    if (c.mat_kind == MAT_NONE) throw BadArg("material not set");
+    if (precision != 0 && precision != 1) throw BadArg("precision must be 0 or 1");
+    if (precision == 1 && !c.K32) dalloc(&c.K32, kKe * c.fine.nel);
+    launch_assemble(c, precision, nullptr);
+    c.assembled = precision;
+    c.mg_prec = c.mg.empty() ? -1 : c.mg_prec;  // hierarchy values are rebuilt on the next solve
+    DP_CUDA(cudaStreamSynchronize(c.stream));
+    return (int)DP_OK;
+  });
+}
+
+int dp_get_element_matrices(dp_ctx* h, double* Ke, double* Ge, double* Me, double* Fb) {
+  if (!h) return DP_BAD_ARG;
+  Ctx& c = h->c;
+  return guarded(&c, [&] {
+    DP_CUDA(cudaSetDevice(c.device));
+    if (c.mat_kind == MAT_NONE) throw BadArg("material not set");
+    const int64_t nel = c.fine.nel;
+    CartOut co;
+    dalloc(&co.Ke, kKe * nel);
+    dalloc(&co.Ge, kGe * nel);
+    dalloc(&co.Me, kMe * nel);
+    dalloc(&co.Fb, kFe * nel);
+    launch_assemble(c, c.assembled == 1 ? 1 : 0, &co);
+    if (Ke) DP_CUDA(cudaMemcpyAsync(Ke, co.Ke, sizeof(double) * kKe * nel, cudaMemcpyDeviceToHost, c.stream));
+    if (Ge) DP_CUDA(cudaMemcpyAsync(Ge, co.Ge, sizeof(double) * kGe * nel, cudaMemcpyDeviceToHost, c.stream));
+    if (Me) DP_CUDA(cudaMemcpyAsync(Me, co.Me, sizeof(double) * kMe * nel, cudaMemcpyDeviceToHost, c.stream));
+    if (Fb) DP_CUDA(cudaMemcpyAsync(Fb, co.Fb, sizeof(double) * kFe * nel, cudaMemcpyDeviceToHost, c.stream));
+    DP_CUDA(cudaStreamSynchronize(c.stream));
+    cudaFree(co.Ke); cudaFree(co.Ge); cudaFree(co.Me); cudaFree(co.Fb);
+    if (c.assembled < 0) c.assembled = 0;
+    return (int)DP_OK;
+  });
+}
+
+int dp_solve(dp_ctx* h, double* U, double* P, double* Ucart, const dp_solve_opts* opts, dp_solve_report* rep,
+             int32_t mem) {
+  if (!h) return DP_BAD_ARG;
+  Ctx& c = h->c;
+  return guarded(&c, [&] {
+    DP_CUDA(cudaSetDevice(c.device));
+    if (!U || !P) throw BadArg("null U or P");
+    if (c.assembled < 0) throw BadArg("dp_assemble must run before dp_solve");
+    SolveCfg cfg = make_cfg(opts);
+    const int64_t nn = c.fine.nnod, np = c.mesh.npres;
+    if (cfg.precision == 1 && c.assembled == 0) {
+      if (!c.K32) dalloc(&c.K32, kKe * c.fine.nel);
+      const int64_t n = kKe * c.fine.nel;
+      k_f64_to_f32<<<(int)div_up(n, 256), 256, 0, c.stream>>>(c.K64, c.K32, n);
+      DP_LAUNCH_CHECK();
+      c.assembled = 1;
+    }
+    cudaEvent_t e0, e1, e2;
+    DP_CUDA(cudaEventCreate(&e0));
+    DP_CUDA(cudaEventCreate(&e1));
+    DP_CUDA(cudaEventCreate(&e2));
+    DP_CUDA(cudaEventRecord(e0, c.stream));
+    mg_setup(c, cfg.precision, cfg.mg);
+    DP_CUDA(cudaEventRecord(e1, c.stream));
+    double* dU = (double*)c.work[W_U];
+    double* dP = (double*)c.work[W_P];
+    if (cfg.use_guess) {
+      DP_CUDA(cudaMemcpyAsync(dP, P, sizeof(double) * np, kind_in(mem), c.stream));
+    }
+    DP_CUDA(cudaMemsetAsync(dU, 0, sizeof(double) * 2 * nn, c.stream));
+    SolveResult res;
+    schur_pcg(c, cfg, dU, dP, res);
+    // lattice -> reference numbering
+    double* stage = (double*)c.work[W_UC];
+    launch_scatter_lat2ref(c, dU, stage, 2);
+    DP_CUDA(cudaMemcpyAsync(U, stage, sizeof(double) * 2 * nn, kind_out(mem), c.stream));
+    DP_CUDA(cudaMemcpyAsync(P, dP, sizeof(double) * np, kind_out(mem), c.stream));
+    if (Ucart) {
+      double* uc = (double*)c.work[W_RES];
+      to_cartesian(c, dU, uc);
+      launch_scatter_lat2ref(c, uc, stage, 2);
+      DP_CUDA(cudaMemcpyAsync(Ucart, stage, sizeof(double) * 2 * nn, kind_out(mem), c.stream));
+    }
+    DP_CUDA(cudaEventRecord(e2, c.stream));
+    DP_CUDA(cudaStreamSynchronize(c.stream));
+    float ms_setup = 0, ms_solve = 0;
+    cudaEventElapsedTime(&ms_setup, e0, e1);
+    cudaEventElapsedTime(&ms_solve, e1, e2);
+    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
+    if (rep) {
+      std::memset(rep, 0, sizeof(*rep));
+      rep->status = res.status;
+      rep->iterations = res.iterations;
+      rep->inner_iterations = res.inner_its;
+      rep->relres = res.relres;
+      rep->r0 = res.r0;
+      rep->omega = res.omega;
+      rep->div_residual = res.div_residual;
+      rep->mom_residual = res.mom_residual;
+      rep->t_setup_ms = ms_setup;
+      rep->t_solve_ms = ms_solve;
+      rep->mg_levels = (int)c.mg.size();
+    }
+    if (res.status == 1) c.err = "outer iteration cap reached";
+    if (res.status == 2) c.err = "breakdown: q.Sq <= 0 or non-finite scalar";
+    return res.status;
+  });
+}
+
+static int apply_common(dp_ctx* h, const double* in, double* out, int32_t mem, int which) {
+  if (!h) return DP_BAD_ARG;
+  Ctx& c = h->c;
+  return guarded(&c, [&] {
+    DP_CUDA(cudaSetDevice(c.device));
+    if (c.assembled < 0) throw BadArg("dp_assemble must run first");
+    if (!in || !out) throw BadArg("null argument");
+    const int64_t nn = c.fine.nnod, np = c.mesh.npres;
+    double* a = (double*)c.work[W_Y];
+    double* b = (double*)c.work[W_Z];
+    double* stage = (double*)c.work[W_UC];
+    double* pbuf = (double*)c.work[W_P];
+    if (which == 0) {  // K
+      DP_CUDA(cudaMemcpyAsync(stage, in, sizeof(double) * 2 * nn, kind_in(mem), c.stream));
+      launch_gather_ref2lat(c, stage, a, 2);
+      launch_apply_K<double, double>(c.fine, c.K64, a, b, c.stream);
+      launch_scatter_lat2ref(c, b, stage, 2);
+      DP_CUDA(cudaMemcpyAsync(out, stage, sizeof(double) * 2 * nn, kind_out(mem), c.stream));
+    } else if (which == 1) {  // G
+      DP_CUDA(cudaMemcpyAsync(pbuf, in, sizeof(double) * np, kind_in(mem), c.stream));
+      launch_apply_G(c, pbuf, b);
+      launch_scatter_lat2ref(c, b, stage, 2);
+      DP_CUDA(cudaMemcpyAsync(out, stage, sizeof(double) * 2 * nn, kind_out(mem), c.stream));
+    } else {  // G^T
+      DP_CUDA(cudaMemcpyAsync(stage, in, sizeof(double) * 2 * nn, kind_in(mem), c.stream));
+      launch_gather_ref2lat(c, stage, a, 2);
+      launch_apply_GT(c, a, pbuf);
+      DP_CUDA(cudaMemcpyAsync(out, pbuf, sizeof(double) * np, kind_out(mem), c.stream));
+    }
+    DP_CUDA(cudaStreamSynchronize(c.stream));
+    return (int)DP_OK;
+  });
+}
+
+int dp_apply_K(dp_ctx* h, const double* x, double* y, int32_t mem) { return apply_common(h, x, y, mem, 0); }
+int dp_apply_G(dp_ctx* h, const double* p, double* y, int32_t mem) { return apply_common(h, p, y, mem, 1); }
+int dp_apply_GT(dp_ctx* h, const double* x, double* p, int32_t mem) { return apply_common(h, x, p, mem, 2); }
+
+int dp_get_rhs(dp_ctx* h, double* F, double* pc) {
+  if (!h) return DP_BAD_ARG;
+  Ctx& c = h->c;
+  return guarded(&c, [&] {
+    DP_CUDA(cudaSetDevice(c.device));
+    if (c.assembled < 0) throw BadArg("dp_assemble must run first");
+    double* stage = (double*)c.work[W_UC];
+    if (F) {
+      launch_scatter_lat2ref(c, c.F, stage, 2);
+      DP_CUDA(cudaMemcpyAsync(F, stage, sizeof(double) * 2 * c.fine.nnod, cudaMemcpyDeviceToHost, c.stream));
+    }
+    if (pc) DP_CUDA(cudaMemcpyAsync(pc, c.pc, sizeof(double) * c.mesh.npres, cudaMemcpyDeviceToHost, c.stream));
+    DP_CUDA(cudaStreamSynchronize(c.stream));
+    return (int)DP_OK;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,191 @@
+// Context, device buffers and shared helpers of the B200 Stokes path.
+//
+// Device data layout (everything lives in HBM for the lifetime of a ctx):
+//   lattice nodes     n = a + A*b, a = 0..2*ncr (radial), b = 0..2*nct-1 (angular,
+//                     periodic); A = 2*ncr+1, B = 2*nct
+//   velocity vectors  interleaved [u_theta, u_r] per lattice node (2*nnod)
+//   pressure          continuous: vertex index (ref numbering = lattice vertex
+//                     (a/2) + (ncr+1)*(b/2)); discontinuous: 3*e + k
+//   element arrays    structure-of-arrays, entry-major: X[k*nel + e]
+//                     (coalesced across consecutive elements)
+//   elements          reference order e = 2*q + t, q = ir + ncr*it,
+//                     connectivity derived from (ir, it, t) -- no index arrays
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "mesh.hpp"
+
+namespace dp {
+
+constexpr int kNip = 6;
+constexpr int kKe = 78;   // packed lower 12x12
+constexpr int kGe = 36;   // 12x3 column-major
+constexpr int kMe = 6;    // packed lower 3x3
+constexpr int kFe = 12;
+
+enum MatKind { MAT_NONE = 0, MAT_ISO = 1, MAT_FULL = 2, MAT_TI = 3 };
+
+// Geometry of one level of the structured hierarchy.
+struct Level {
+  int ncr = 0, nct = 0;
+  int pin = 0;               // u_theta of lattice node (2*ncr, 0) is fixed
+  int64_t nel = 0, nnod = 0;
+  int64_t A() const { return 2 * (int64_t)ncr + 1; }
+  int64_t B() const { return 2 * (int64_t)nct; }
+};
+
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+};
+
+struct MGLevel {
+  Level g;
+  double* K64 = nullptr;     // 78*nel packed polar, masked
+  float* K32 = nullptr;
+  double* dinv64 = nullptr;  // 2*nnod inverse diagonal (0 on fixed DOFs)
+  float* dinv32 = nullptr;
+  double lmax = 0.0;         // estimate of lambda_max(D^-1 A)
+  // work vectors (precision of the hierarchy)
+  void* x = nullptr;
+  void* b = nullptr;
+  void* r = nullptr;
+  void* d = nullptr;
+  void* t = nullptr;
+};
+
+struct Ctx {
+  Mesh mesh;
+  Level fine;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+
+  // geometry
+  double* theta_lat = nullptr;  // nnod
+  double* r_lat = nullptr;      // nnod
+  int64_t* ref2lat = nullptr;   // nnod
+
+  // material
+  int mat_kind = MAT_NONE;
+  double g = 0.0;
+  double* eta = nullptr;        // 6*nel (ip-major)
+  double* C = nullptr;          // FULL: 36*nel (field*6+ip); TI: 3*nel (delta, dx, dy)
+  double* rho_lat = nullptr;    // nnod
+  double* rho_ref = nullptr;    // nnod (reference numbering, for uploads)
+
+  // assembled (polar, masked)
+  int assembled = -1;           // precision of the last assembly, -1 = none
+  double* K64 = nullptr;        // 78*nel
+  float* K32 = nullptr;         // 78*nel (refined path)
+  double* Gp = nullptr;         // 36*nel
+  double* F = nullptr;          // 2*nnod
+  double* pc = nullptr;         // npres (1/rowsum M)
+  double* Fscale = nullptr;
+
+  // multigrid hierarchy (level 0 = fine)
+  std::vector<MGLevel> mg;
+  int mg_prec = -1;             // 0 = fp64, 1 = fp32
+  double* coarse_chol = nullptr;// dense Cholesky factor of the coarsest level
+  int64_t coarse_n = 0;
+  int64_t* coarse_map = nullptr;// coarsest DOF -> dense index (-1 fixed)
+
+  // scratch
+  double* scal = nullptr;       // device scalars
+  double* h_scal = nullptr;     // pinned host mirror
+  double* partial = nullptr;    // reduction partials
+  unsigned int* counter = nullptr;
+  std::vector<void*> work;      // solver vectors
+
+  ~Ctx();
+};
+
+// ---- error handling --------------------------------------------------------
+struct CudaError {
+  cudaError_t e;
+  const char* what;
+  int line;
+};
+
+#define DP_CUDA(call)                                             \
+  do {                                                            \
+    cudaError_t e__ = (call);                                     \
+    if (e__ != cudaSuccess) throw ::dp::CudaError{e__, #call, __LINE__}; \
+  } while (0)
+
+#define DP_LAUNCH_CHECK() DP_CUDA(cudaGetLastError())
+
+// ---- lattice helpers (host + device) ---------------------------------------
+// Constrained DOFs: u_r on both walls (free slip, boundary_conditions.jl:27-37)
+// and, when pinned, u_theta of the outer-wall node at theta = 0 (the one-node
+// tangential constraint of free_slip(nr, ids), boundary_conditions.jl:180-194).
+__host__ __device__ inline bool dof_fixed(int a, int b, int comp, int amax, int pin) {
+  if (comp == 1) return a == 0 || a == amax;
+  return pin && a == amax && b == 0;
+}
+
+__host__ __device__ inline int64_t wrapb(int64_t b, int64_t B) { return b >= B ? b - B : (b < 0 ? b + B : b); }
+
+// Lattice (a, b) of the 6 local nodes of element e on a level with ncr radial cells.
+__host__ __device__ inline void element_nodes(int64_t e, int ncr, int64_t A, int64_t B, int64_t n[6]) {
+  const int64_t q = e >> 1;
+  const int t = (int)(e & 1);
+  const int64_t ir = q % ncr, it = q / ncr;
+  const int64_t a0 = 2 * ir, b0 = 2 * it;
+  int64_t a[6], b[6];
+  if (t == 0) {  // [v1, v2, v4]
+    a[0] = a0;     b[0] = b0;
+    a[1] = a0;     b[1] = b0 + 2;
+    a[2] = a0 + 2; b[2] = b0;
+    a[3] = a0;     b[3] = b0 + 1;
+    a[4] = a0 + 1; b[4] = b0 + 1;
+    a[5] = a0 + 1; b[5] = b0;
+  } else {       // [v2, v3, v4]
+    a[0] = a0;     b[0] = b0 + 2;
+    a[1] = a0 + 2; b[1] = b0 + 2;
+    a[2] = a0 + 2; b[2] = b0;
+    a[3] = a0 + 1; b[3] = b0 + 2;
+    a[4] = a0 + 2; b[4] = b0 + 1;
+    a[5] = a0 + 1; b[5] = b0 + 1;
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) n[k] = a[k] + A * wrapb(b[k], B);
+}
+
+__host__ __device__ inline void element_pdofs_cont(int64_t e, int ncr, int nct, int64_t p[3]) {
+  const int64_t q = e >> 1;
+  const int t = (int)(e & 1);
+  const int64_t ir = q % ncr, it = q / ncr;
+  const int64_t nr = ncr + 1;
+  const int64_t it1 = (it + 1 == nct) ? 0 : it + 1;
+  const int64_t v1 = ir + nr * it, v2 = ir + nr * it1, v3 = ir + 1 + nr * it1, v4 = ir + 1 + nr * it;
+  if (t == 0) { p[0] = v1; p[1] = v2; p[2] = v4; }
+  else        { p[0] = v2; p[1] = v3; p[2] = v4; }
+}
+
+// Pressure DOFs of element e: continuous = vertex numbering (EL2NOD[1:3,:],
+// mesher.jl:213); discontinuous = 3e+k (reshape(1:3nel,3,nel), mesher.jl:212).
+__host__ __device__ inline void element_pdofs(int64_t e, int ncr, int nct, int pressure, int64_t p[3]) {
+  if (pressure == 1) {
+    p[0] = 3 * e; p[1] = 3 * e + 1; p[2] = 3 * e + 2;
+  } else {
+    element_pdofs_cont(e, ncr, nct, p);
+  }
+}
+
+// Packed lower-column-major index of the 12x12 element matrix entry (R >= C);
+// the reference's loops emit Ke in this order (StokesSolver.jl:696-741).
+__host__ __device__ constexpr int packed_index12(int R, int C) {
+  // R >= C; column-major lower packing of a 12x12 matrix
+  return C * 12 - (C * (C - 1)) / 2 + (R - C);
+}
+
+inline int64_t div_up(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+}  // namespace dp

@@ -1,0 +1,8 @@
+// Single translation unit of the device library: the kernels share their
+// __constant__ tables (quadrature, multigrid child maps) without relocatable
+// device code.
+#include "assemble.cu"
+#include "ops.cu"
+#include "mg.cu"
+#include "solver.cu"
+#include "capi.cu"

@@ -1,0 +1,660 @@
+// Geometric multigrid preconditioner for the velocity block K (free DOFs).
+//
+// The reference inverts K[ifree, ifree] with a sparse LU once per solve and
+// back-substitutes per outer iteration (src/PardisoSolvers.jl:247-256,
+// :274-278).  On the device the inner solve is PCG preconditioned by one
+// V-cycle of this hierarchy.
+//
+// Hierarchy.  The split-1 annulus with (ncr, nct) cells is nested in the one
+// with (ncr/2, nct/2) cells: every coarse triangle is the union of 4 fine
+// triangles and the fine diagonals continue the coarse ones, so coarse P2 is a
+// subspace of fine P2 in (theta, r).  Prolongation P interpolates each polar
+// component with the coarse P2 basis.  Coarse operators are Galerkin,
+// A_c = P^T A P, computed element by element: K_E = sum_{children f}
+// P_f^T K_f P_f with the 6x6 local interpolation P_f of each child position,
+// followed by the coarse free-slip mask.  This keeps every level in the same
+// packed element-by-element form as the fine level.
+// Smoother: Chebyshev polynomial in D^-1 A (point Jacobi), bounds from a
+// 10-step CG-Lanczos estimate of lambda_max.  Coarsest level: dense Cholesky,
+// inverted once per setup and applied as a dense mat-vec.
+#include <algorithm>
+#include <cmath>
+
+#include "kernels.cuh"
+#include "mg.cuh"
+
+namespace dp {
+
+// ---- host-side constant tables ---------------------------------------------
+struct ChildTable {
+  int dr[2][4], dt[2][4], tf[2][4];  // child cell offset (radial, angular) and type
+  double P[2][4][6][6];              // P[coarse type][child][fine local][coarse local]
+};
+__constant__ ChildTable c_child;
+
+static void p2_values(double xi, double eta, double N[6]) {
+  const double t = 1.0 - xi - eta;
+  N[0] = t * (2.0 * t - 1.0);
+  N[1] = xi * (2.0 * xi - 1.0);
+  N[2] = eta * (2.0 * eta - 1.0);
+  N[3] = 4.0 * xi * t;
+  N[4] = 4.0 * xi * eta;
+  N[5] = 4.0 * eta * t;
+}
+
+// Local node offsets (radial a, angular b) of the 6 nodes of a triangle of type t
+// inside its cell, in units of the P2 lattice of that level.
+static const int kLocA[2][6] = {{0, 0, 2, 0, 1, 1}, {0, 2, 2, 1, 2, 1}};
+static const int kLocB[2][6] = {{0, 2, 0, 1, 1, 0}, {2, 2, 0, 2, 1, 1}};
+
+// Coarse reference coordinates of a point given in fine-lattice offsets
+// (alpha radial, beta angular) from the coarse cell origin (coarse cell = 4x4).
+static void coarse_ref(int type, double alpha, double beta, double* xi, double* eta) {
+  if (type == 0) {  // v1 (0,0), v2 (0,4), v3 (4,0): point = (4 eta, 4 xi)
+    *xi = beta / 4.0;
+    *eta = alpha / 4.0;
+  } else {          // v1 (0,4), v2 (4,4), v3 (4,0): point = (4 xi + 4 eta, 4 - 4 eta)
+    *eta = (4.0 - beta) / 4.0;
+    *xi = (alpha + beta - 4.0) / 4.0;
+  }
+}
+
+void upload_mg_constants() {
+  ChildTable T{};
+  // coarse A children: (0,0,A) (0,0,B) (0,1,A) (1,0,A); coarse B: (0,1,B) (1,0,B) (1,1,A) (1,1,B)
+  const int dr[2][4] = {{0, 0, 0, 1}, {0, 1, 1, 1}};
+  const int dt[2][4] = {{0, 0, 1, 0}, {1, 0, 1, 1}};
+  const int tf[2][4] = {{0, 1, 0, 0}, {1, 1, 0, 1}};
+  for (int ct = 0; ct < 2; ++ct)
+    for (int ch = 0; ch < 4; ++ch) {
+      T.dr[ct][ch] = dr[ct][ch];
+      T.dt[ct][ch] = dt[ct][ch];
+      T.tf[ct][ch] = tf[ct][ch];
+      for (int i = 0; i < 6; ++i) {
+        const double alpha = 2 * dr[ct][ch] + kLocA[tf[ct][ch]][i];
+        const double beta = 2 * dt[ct][ch] + kLocB[tf[ct][ch]][i];
+        double xi, eta, N[6];
+        coarse_ref(ct, alpha, beta, &xi, &eta);
+        p2_values(xi, eta, N);
+        for (int k = 0; k < 6; ++k) T.P[ct][ch][i][k] = N[k];
+      }
+    }
+  DP_CUDA(cudaMemcpyToSymbol(c_child, &T, sizeof(T)));
+}
+
+// ---- Galerkin coarsening: one thread per (coarse element, packed entry) ------
+template <typename T>
+__global__ void k_galerkin(const T* __restrict__ Kf, T* __restrict__ Kc, int nelc, int ncrc, int nctc, int nelf,
+                           int ncrf, int pin) {
+  const int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (gid >= (int64_t)nelc * kKe) return;
+  const int E = (int)(gid % nelc);
+  const int pidx = (int)(gid / nelc);
+  // decode packed index -> (R, C)
+  int C = 0, off = 0;
+  while (off + (12 - C) <= pidx) { off += 12 - C; ++C; }
+  const int R = C + (pidx - off);
+  const int k = R >> 1, alpha = R & 1, l = C >> 1, beta = C & 1;
+  const int Q = E >> 1, ct = E & 1;
+  const int IR = Q % ncrc, IT = Q / ncrc;
+  double acc = 0.0;
+#pragma unroll
+  for (int ch = 0; ch < 4; ++ch) {
+    const int fr = 2 * IR + c_child.dr[ct][ch], ft = 2 * IT + c_child.dt[ct][ch];
+    const int ef = 2 * (fr + ncrf * ft) + c_child.tf[ct][ch];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      const double pik = c_child.P[ct][ch][i][k];
+      if (pik == 0.0) continue;
+      double s = 0.0;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        const double pjl = c_child.P[ct][ch][j][l];
+        if (pjl == 0.0) continue;
+        const int r = 2 * i + alpha, cc = 2 * j + beta;
+        const int pi = r >= cc ? packed_index12(r, cc) : packed_index12(cc, r);
+        s += pjl * (double)Kf[(size_t)pi * nelf + ef];
+      }
+      acc += pik * s;
+    }
+  }
+  // coarse constraint mask (free slip + optional tangential pin)
+  const int a0 = 2 * IR, b0 = 2 * IT, Bc = 2 * nctc;
+  const int ak = a0 + kLocA_dev(ct, k), al = a0 + kLocA_dev(ct, l);
+  int bk = b0 + kLocB_dev(ct, k), bl = b0 + kLocB_dev(ct, l);
+  if (bk >= Bc) bk -= Bc;
+  if (bl >= Bc) bl -= Bc;
+  const int amax = 2 * ncrc;
+  if (dof_fixed(ak, bk, alpha, amax, pin) || dof_fixed(al, bl, beta, amax, pin)) acc = 0.0;
+  Kc[(size_t)pidx * nelc + E] = (T)acc;
+}
+
+// ---- diagonal --------------------------------------------------------------
+template <typename T>
+__global__ void k_diag(const T* __restrict__ K, double* __restrict__ diag, int nel, int ncr, int A, int B) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nel) return;
+  int nd[6];
+  element_nodes_mg(e, ncr, A, B, nd);
+#pragma unroll
+  for (int d = 0; d < 12; ++d) atomicAdd(&diag[2 * nd[d >> 1] + (d & 1)], (double)K[(size_t)packed_index12(d, d) * nel + e]);
+}
+
+template <typename T>
+__global__ void k_diag_invert(const double* __restrict__ diag, T* __restrict__ dinv, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double d = diag[i];
+  dinv[i] = (T)(d > 0.0 ? 1.0 / d : 0.0);
+}
+
+// ---- transfers ---------------------------------------------------------------
+// Fine node (a, b) -> containing coarse element and the 6 coarse P2 weights.
+__device__ inline void fine_node_weights(int a, int b, int ncrc, int Ac, int Bc, int cn[6], double w[6]) {
+  int IR = a >> 2;
+  if (IR >= ncrc) IR = ncrc - 1;
+  const int IT = b >> 2;
+  const int alpha = a - 4 * IR, beta = b - 4 * IT;
+  const int ct = (alpha + beta <= 4) ? 0 : 1;
+  double xi, eta;
+  if (ct == 0) { xi = beta * 0.25; eta = alpha * 0.25; }
+  else { eta = (4 - beta) * 0.25; xi = (alpha + beta - 4) * 0.25; }
+  const double t = 1.0 - xi - eta;
+  w[0] = t * (2.0 * t - 1.0);
+  w[1] = xi * (2.0 * xi - 1.0);
+  w[2] = eta * (2.0 * eta - 1.0);
+  w[3] = 4.0 * xi * t;
+  w[4] = 4.0 * xi * eta;
+  w[5] = 4.0 * eta * t;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const int ac = 2 * IR + kLocA_dev(ct, k);
+    int bc = 2 * IT + kLocB_dev(ct, k);
+    if (bc >= Bc) bc -= Bc;
+    cn[k] = ac + Ac * bc;
+  }
+}
+
+// xf += P xc (per fine node, gather)
+template <typename T>
+__global__ void k_prolong_add(const T* __restrict__ xc, T* __restrict__ xf, int Af, int Bf, int ncrc, int Ac, int Bc,
+                              int pin) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= Af * Bf) return;
+  const int a = n % Af, b = n / Af;
+  int cn[6];
+  double w[6];
+  fine_node_weights(a, b, ncrc, Ac, Bc, cn, w);
+  double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    if (w[k] != 0.0) {
+      s0 += w[k] * (double)xc[2 * cn[k]];
+      s1 += w[k] * (double)xc[2 * cn[k] + 1];
+    }
+  }
+  if (!dof_fixed(a, b, 0, Af - 1, pin)) xf[2 * n] += (T)s0;
+  if (!dof_fixed(a, b, 1, Af - 1, pin)) xf[2 * n + 1] += (T)s1;
+}
+
+// bc = P^T rf (per fine node scatter), bc zeroed by the caller
+template <typename T>
+__global__ void k_restrict(const T* __restrict__ rf, T* __restrict__ bc, int Af, int Bf, int ncrc, int Ac, int Bc,
+                           int pin) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= Af * Bf) return;
+  const int a = n % Af, b = n / Af;
+  int cn[6];
+  double w[6];
+  fine_node_weights(a, b, ncrc, Ac, Bc, cn, w);
+  const double r0 = dof_fixed(a, b, 0, Af - 1, pin) ? 0.0 : (double)rf[2 * n];
+  const double r1 = dof_fixed(a, b, 1, Af - 1, pin) ? 0.0 : (double)rf[2 * n + 1];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    if (w[k] != 0.0) {
+      atomicAdd(&bc[2 * cn[k]], (T)(w[k] * r0));
+      atomicAdd(&bc[2 * cn[k] + 1], (T)(w[k] * r1));
+    }
+  }
+}
+
+// zero the constrained DOFs: wall u_r (2*B of them) and the pinned u_theta
+template <typename T>
+__global__ void k_mask_fixed(T* __restrict__ v, int A, int B, int pin) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n == 2 * B) {
+    if (pin) v[2 * (A - 1)] = (T)0;
+    return;
+  }
+  if (n > 2 * B) return;
+  const int b = n >> 1;
+  const int a = (n & 1) ? A - 1 : 0;
+  v[2 * (a + A * b) + 1] = (T)0;
+}
+
+// ---- Chebyshev smoother vector steps -----------------------------------------
+// first step from x = 0: r = b, d = (1/theta) D^-1 b, x = d
+template <typename T>
+__global__ void k_cheb_first(const T* __restrict__ b, const T* __restrict__ dinv, T* __restrict__ x,
+                             T* __restrict__ r, T* __restrict__ d, double inv_theta, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const T bi = b[i];
+  const T di = (T)(inv_theta * (double)dinv[i] * (double)bi);
+  r[i] = bi;
+  d[i] = di;
+  x[i] = di;
+}
+// first step from a given x: r = b - Ax (Ax in r on entry), d = (1/theta) D^-1 r, x += d
+template <typename T>
+__global__ void k_cheb_first_x(const T* __restrict__ b, const T* __restrict__ dinv, T* __restrict__ x,
+                               T* __restrict__ r, T* __restrict__ d, double inv_theta, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const T ri = b[i] - r[i];
+  const T di = (T)(inv_theta * (double)dinv[i] * (double)ri);
+  r[i] = ri;
+  d[i] = di;
+  x[i] += di;
+}
+// r -= Ad; d = c1 d + c2 D^-1 r; x += d
+template <typename T>
+__global__ void k_cheb_step(const T* __restrict__ Ad, const T* __restrict__ dinv, T* __restrict__ x,
+                            T* __restrict__ r, T* __restrict__ d, double c1, double c2, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const T ri = r[i] - Ad[i];
+  const T di = (T)(c1 * (double)d[i] + c2 * (double)dinv[i] * (double)ri);
+  r[i] = ri;
+  d[i] = di;
+  x[i] += di;
+}
+template <typename T>
+__global__ void k_sub(const T* __restrict__ b, T* __restrict__ r, int64_t n) {  // r = b - r
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) r[i] = b[i] - r[i];
+}
+
+// ---- coarse dense solve --------------------------------------------------------
+template <typename T>
+__global__ void k_dense_assemble(const T* __restrict__ K, double* __restrict__ D, int nel, int ncr, int A, int B, int n) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nel) return;
+  int nd[6];
+  element_nodes_mg(e, ncr, A, B, nd);
+  for (int C = 0; C < 12; ++C)
+    for (int R = C; R < 12; ++R) {
+      const double v = (double)K[(size_t)packed_index12(R, C) * nel + e];
+      const int gr = 2 * nd[R >> 1] + (R & 1), gc = 2 * nd[C >> 1] + (C & 1);
+      atomicAdd(&D[(size_t)gr * n + gc], v);
+      if (R != C) atomicAdd(&D[(size_t)gc * n + gr], v);
+    }
+}
+
+// identity on fixed (zero) rows, then in-place Cholesky (lower) in one CTA
+__global__ void k_dense_cholesky(double* __restrict__ D, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    if (D[(size_t)i * n + i] == 0.0) D[(size_t)i * n + i] = 1.0;
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    if (threadIdx.x == 0) D[(size_t)k * n + k] = sqrt(D[(size_t)k * n + k]);
+    __syncthreads();
+    const double dk = D[(size_t)k * n + k];
+    for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x) D[(size_t)i * n + k] /= dk;
+    __syncthreads();
+    const int m = n - k - 1;
+    for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
+      const int i = k + 1 + idx / m, j = k + 1 + idx % m;
+      if (j <= i) D[(size_t)i * n + j] -= D[(size_t)i * n + k] * D[(size_t)j * n + k];
+    }
+    __syncthreads();
+  }
+}
+
+// Inverse from the Cholesky factor: column c of A^-1 by forward + back substitution.
+__global__ void k_dense_inverse(const double* __restrict__ L, double* __restrict__ Inv, double* __restrict__ tmp, int n) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  double* y = tmp + (size_t)c * n;
+  for (int i = 0; i < n; ++i) {
+    double s = (i == c) ? 1.0 : 0.0;
+    for (int j = 0; j < i; ++j) s -= L[(size_t)i * n + j] * y[j];
+    y[i] = s / L[(size_t)i * n + i];
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    double s = y[i];
+    for (int j = i + 1; j < n; ++j) s -= L[(size_t)j * n + i] * y[j];
+    y[i] = s / L[(size_t)i * n + i];
+  }
+  for (int i = 0; i < n; ++i) Inv[(size_t)i * n + c] = y[i];
+}
+
+template <typename T>
+__global__ void k_dense_apply(const double* __restrict__ Inv, const T* __restrict__ b, T* __restrict__ x, int n) {
+  const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  double s = 0.0;
+  for (int j = lane; j < n; j += 32) s += Inv[(size_t)row * n + j] * (double)b[j];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) x[row] = (T)s;
+}
+
+// ---- host side ---------------------------------------------------------------
+static int tpb(int64_t n) { return (int)div_up(n, 256); }
+
+template <typename T>
+static T* level_K(MGLevel& L);
+template <>
+double* level_K<double>(MGLevel& L) { return L.K64; }
+template <>
+float* level_K<float>(MGLevel& L) { return L.K32; }
+template <typename T>
+static T* level_dinv(MGLevel& L);
+template <>
+double* level_dinv<double>(MGLevel& L) { return L.dinv64; }
+template <>
+float* level_dinv<float>(MGLevel& L) { return L.dinv32; }
+
+void mg_free(Ctx& c) {
+  for (size_t l = 0; l < c.mg.size(); ++l) {
+    MGLevel& L = c.mg[l];
+    if (l > 0) { cudaFree(L.K64); cudaFree(L.K32); }
+    cudaFree(L.dinv64); cudaFree(L.dinv32);
+    cudaFree(L.x); cudaFree(L.b); cudaFree(L.r); cudaFree(L.d); cudaFree(L.t);
+  }
+  c.mg.clear();
+  cudaFree(c.coarse_chol);
+  c.coarse_chol = nullptr;
+  c.coarse_n = 0;
+  c.mg_prec = -1;
+}
+
+// Largest eigenvalue of a symmetric tridiagonal matrix (Sturm bisection).
+static double tridiag_lmax(const std::vector<double>& a, const std::vector<double>& b) {
+  const int m = (int)a.size();
+  double lo = 0.0, hi = 0.0;
+  for (int i = 0; i < m; ++i) {
+    const double r = (i > 0 ? std::fabs(b[i - 1]) : 0.0) + (i < m - 1 ? std::fabs(b[i]) : 0.0);
+    hi = std::max(hi, a[i] + r);
+    lo = std::min(lo, a[i] - r);
+  }
+  auto count_below = [&](double x) {
+    int cnt = 0;
+    double d = 1.0;
+    for (int i = 0; i < m; ++i) {
+      d = a[i] - x - (i > 0 ? b[i - 1] * b[i - 1] / d : 0.0);
+      if (d == 0.0) d = 1e-300;
+      if (d < 0) ++cnt;
+    }
+    return cnt;
+  };
+  for (int it = 0; it < 100; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (count_below(mid) >= m) hi = mid; else lo = mid;
+  }
+  return hi;
+}
+
+template <typename T>
+static void apply_level(Ctx& c, MGLevel& L, const T* x, T* y) {
+  launch_apply_K<T, T>(L.g, level_K<T>(L), x, y, c.stream);
+}
+
+template <typename T>
+static void dot_level(Ctx& c, const T* a, const T* b, int64_t n, int slot);
+template <>
+void dot_level<double>(Ctx& c, const double* a, const double* b, int64_t n, int slot) { launch_dot(c, a, b, n, slot); }
+template <>
+void dot_level<float>(Ctx& c, const float* a, const float* b, int64_t n, int slot) { launch_dot_f(c, a, b, n, slot); }
+
+template <typename T>
+__global__ void k_fill_pattern(T* v, int64_t n, int A, int pin) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  // deterministic pseudo-random start vector, zero on fixed DOFs
+  uint64_t z = (uint64_t)i * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+  const int64_t node = i >> 1;
+  const int a = (int)(node % A), b = (int)(node / A);
+  const bool fixed = dof_fixed(a, b, (int)(i & 1), A - 1, pin);
+  v[i] = fixed ? (T)0 : (T)u;
+}
+
+template <typename T>
+__global__ void k_pcg_vec(T* __restrict__ x, T* __restrict__ r, T* __restrict__ p, const T* __restrict__ Ap,
+                          const T* __restrict__ dinv, T* __restrict__ z, double alpha, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] += (T)(alpha * (double)p[i]);
+  const T ri = r[i] - (T)(alpha * (double)Ap[i]);
+  r[i] = ri;
+  z[i] = dinv[i] * ri;
+}
+template <typename T>
+__global__ void k_xpby(const T* __restrict__ z, T* __restrict__ p, double beta, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) p[i] = z[i] + (T)(beta * (double)p[i]);
+}
+template <typename T>
+__global__ void k_mul(const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ out, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a[i] * b[i];
+}
+
+// lambda_max(D^-1 A) from 10 steps of Jacobi-PCG (Lanczos coefficients).
+template <typename T>
+static double estimate_lmax(Ctx& c, MGLevel& L) {
+  const int64_t n = 2 * L.g.nnod;
+  T* x = (T*)L.x; T* r = (T*)L.r; T* p = (T*)L.d; T* z = (T*)L.b; T* Ap = (T*)L.t;
+  const T* dinv = level_dinv<T>(L);
+  DP_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * n, c.stream));
+  k_fill_pattern<T><<<tpb(n), 256, 0, c.stream>>>(r, n, (int)L.g.A(), L.g.pin);
+  k_mul<T><<<tpb(n), 256, 0, c.stream>>>(dinv, r, z, n);
+  DP_CUDA(cudaMemcpyAsync(p, z, sizeof(T) * n, cudaMemcpyDeviceToDevice, c.stream));
+  dot_level<T>(c, r, z, n, 20);
+  DP_CUDA(cudaMemcpyAsync(c.h_scal + 20, c.scal + 20, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  DP_CUDA(cudaStreamSynchronize(c.stream));
+  double rz = c.h_scal[20];
+  std::vector<double> alphas, betas;
+  const int kSteps = 10;
+  for (int k = 0; k < kSteps && rz > 0.0; ++k) {
+    apply_level<T>(c, L, p, Ap);
+    dot_level<T>(c, p, Ap, n, 21);
+    DP_CUDA(cudaMemcpyAsync(c.h_scal + 21, c.scal + 21, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    DP_CUDA(cudaStreamSynchronize(c.stream));
+    const double pAp = c.h_scal[21];
+    if (!(pAp > 0.0)) break;
+    const double alpha = rz / pAp;
+    k_pcg_vec<T><<<tpb(n), 256, 0, c.stream>>>(x, r, p, Ap, dinv, z, alpha, n);
+    dot_level<T>(c, r, z, n, 20);
+    DP_CUDA(cudaMemcpyAsync(c.h_scal + 20, c.scal + 20, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    DP_CUDA(cudaStreamSynchronize(c.stream));
+    const double rz_new = c.h_scal[20];
+    const double beta = rz_new / rz;
+    alphas.push_back(alpha);
+    betas.push_back(beta);
+    rz = rz_new;
+    if (!(rz > 0.0)) break;
+    k_xpby<T><<<tpb(n), 256, 0, c.stream>>>(z, p, beta, n);
+  }
+  DP_LAUNCH_CHECK();
+  const int m = (int)alphas.size();
+  if (m == 0) return 2.0;
+  std::vector<double> a(m), b(std::max(m - 1, 0));
+  for (int j = 0; j < m; ++j) {
+    a[j] = 1.0 / alphas[j] + (j > 0 ? betas[j - 1] / alphas[j - 1] : 0.0);
+    if (j < m - 1) b[j] = std::sqrt(betas[j]) / alphas[j];
+  }
+  return tridiag_lmax(a, b);
+}
+
+template <typename T>
+static void setup_level_vectors(MGLevel& L) {
+  const size_t bytes = sizeof(T) * 2 * L.g.nnod;
+  DP_CUDA(cudaMalloc(&L.x, bytes));
+  DP_CUDA(cudaMalloc(&L.b, bytes));
+  DP_CUDA(cudaMalloc(&L.r, bytes));
+  DP_CUDA(cudaMalloc(&L.d, bytes));
+  DP_CUDA(cudaMalloc(&L.t, bytes));
+}
+
+template <typename T>
+static void mg_setup_t(Ctx& c, const MGOptions& o) {
+  const int prec = std::is_same<T, float>::value ? 1 : 0;
+  // level geometry (reuse if unchanged)
+  if (c.mg.empty() || c.mg_prec != prec) {
+    mg_free(c);
+    MGLevel L0;
+    L0.g = c.fine;
+    c.mg.push_back(L0);
+    while (true) {
+      const Level& g = c.mg.back().g;
+      if (g.ncr % 2 || g.nct % 2 || g.nct / 2 < 4) break;
+      if ((int)c.mg.size() >= o.max_levels) break;
+      Level h;
+      h.ncr = g.ncr / 2;
+      h.nct = g.nct / 2;
+      h.nel = 2 * (int64_t)h.ncr * h.nct;
+      h.nnod = h.A() * h.B();
+      h.pin = g.pin;
+      if (2 * g.nnod <= o.coarse_max) break;
+      MGLevel Lh;
+      Lh.g = h;
+      c.mg.push_back(Lh);
+    }
+    for (size_t l = 0; l < c.mg.size(); ++l) {
+      MGLevel& L = c.mg[l];
+      if (l > 0) {
+        DP_CUDA(cudaMalloc(prec ? (void**)&L.K32 : (void**)&L.K64, sizeof(T) * kKe * L.g.nel));
+      }
+      DP_CUDA(cudaMalloc(prec ? (void**)&L.dinv32 : (void**)&L.dinv64, sizeof(T) * 2 * L.g.nnod));
+      setup_level_vectors<T>(L);
+    }
+    c.coarse_n = 2 * c.mg.back().g.nnod;
+    if (c.coarse_n <= o.coarse_max) {
+      DP_CUDA(cudaMalloc(&c.coarse_chol, sizeof(double) * c.coarse_n * c.coarse_n * 3));
+    } else {
+      c.coarse_n = 0;
+    }
+    c.mg_prec = prec;
+  }
+  // fine operator pointer
+  if (prec) c.mg[0].K32 = c.K32; else c.mg[0].K64 = c.K64;
+  // Galerkin coarse operators
+  for (size_t l = 1; l < c.mg.size(); ++l) {
+    MGLevel& Lf = c.mg[l - 1];
+    MGLevel& Lc = c.mg[l];
+    const int64_t nthreads = Lc.g.nel * kKe;
+    k_galerkin<T><<<(int)div_up(nthreads, 128), 128, 0, c.stream>>>(level_K<T>(Lf), level_K<T>(Lc), (int)Lc.g.nel,
+                                                                      Lc.g.ncr, Lc.g.nct, (int)Lf.g.nel, Lf.g.ncr,
+                                                                      Lc.g.pin);
+    DP_LAUNCH_CHECK();
+  }
+  // diagonals + eigenvalue estimates
+  double* diag = nullptr;
+  DP_CUDA(cudaMalloc(&diag, sizeof(double) * 2 * c.mg[0].g.nnod));
+  for (size_t l = 0; l < c.mg.size(); ++l) {
+    MGLevel& L = c.mg[l];
+    const int64_t n = 2 * L.g.nnod;
+    DP_CUDA(cudaMemsetAsync(diag, 0, sizeof(double) * n, c.stream));
+    k_diag<T><<<(int)div_up(L.g.nel, 128), 128, 0, c.stream>>>(level_K<T>(L), diag, (int)L.g.nel, L.g.ncr,
+                                                                (int)L.g.A(), (int)L.g.B());
+    k_diag_invert<T><<<tpb(n), 256, 0, c.stream>>>(diag, level_dinv<T>(L), n);
+    DP_LAUNCH_CHECK();
+    const bool is_coarsest_direct = (l + 1 == c.mg.size()) && c.coarse_n > 0;
+    L.lmax = is_coarsest_direct ? 0.0 : estimate_lmax<T>(c, L);
+  }
+  DP_CUDA(cudaFree(diag));
+  // coarse dense inverse
+  if (c.coarse_n > 0) {
+    MGLevel& L = c.mg.back();
+    const int n = (int)c.coarse_n;
+    double* D = c.coarse_chol;
+    double* Inv = D + (size_t)n * n;
+    double* tmp = Inv + (size_t)n * n;
+    DP_CUDA(cudaMemsetAsync(D, 0, sizeof(double) * n * n, c.stream));
+    k_dense_assemble<T><<<(int)div_up(L.g.nel, 128), 128, 0, c.stream>>>(level_K<T>(L), D, (int)L.g.nel, L.g.ncr,
+                                                                          (int)L.g.A(), (int)L.g.B(), n);
+    k_dense_cholesky<<<1, 1024, 0, c.stream>>>(D, n);
+    k_dense_inverse<<<(int)div_up(n, 64), 64, 0, c.stream>>>(D, Inv, tmp, n);
+    DP_LAUNCH_CHECK();
+  }
+}
+
+void mg_setup(Ctx& c, int precision, const MGOptions& o) {
+  if (precision == 1) mg_setup_t<float>(c, o);
+  else mg_setup_t<double>(c, o);
+}
+
+// Chebyshev smoothing of A x = b on level L; x_zero: start from x = 0.
+template <typename T>
+static void chebyshev(Ctx& c, MGLevel& L, const T* b, T* x, bool x_zero, const MGOptions& o) {
+  const int64_t n = 2 * L.g.nnod;
+  const double lmax = o.cheb_hi * L.lmax, lmin = o.cheb_lo * L.lmax;
+  const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
+  const double sigma = theta / delta;
+  double rho_prev = 1.0 / sigma;
+  T* r = (T*)L.r; T* d = (T*)L.d; T* Ad = (T*)L.t;
+  const T* dinv = level_dinv<T>(L);
+  if (x_zero) {
+    k_cheb_first<T><<<tpb(n), 256, 0, c.stream>>>(b, dinv, x, r, d, 1.0 / theta, n);
+  } else {
+    apply_level<T>(c, L, x, r);
+    k_cheb_first_x<T><<<tpb(n), 256, 0, c.stream>>>(b, dinv, x, r, d, 1.0 / theta, n);
+  }
+  for (int k = 1; k < o.cheb_degree; ++k) {
+    apply_level<T>(c, L, d, Ad);
+    const double rho = 1.0 / (2.0 * sigma - rho_prev);
+    k_cheb_step<T><<<tpb(n), 256, 0, c.stream>>>(Ad, dinv, x, r, d, rho * rho_prev, 2.0 * rho / delta, n);
+    rho_prev = rho;
+  }
+  DP_LAUNCH_CHECK();
+}
+
+template <typename T>
+static void vcycle(Ctx& c, size_t l, const T* b, T* x, const MGOptions& o) {
+  MGLevel& L = c.mg[l];
+  const int64_t n = 2 * L.g.nnod;
+  if (l + 1 == c.mg.size()) {
+    if (c.coarse_n > 0) {
+      const int nn = (int)c.coarse_n;
+      const double* Inv = c.coarse_chol + (size_t)nn * nn;
+      k_dense_apply<T><<<(int)div_up(nn, 8), 256, 0, c.stream>>>(Inv, b, x, nn);
+      k_mask_fixed<T><<<tpb(2 * L.g.B() + 1), 256, 0, c.stream>>>(x, (int)L.g.A(), (int)L.g.B(), L.g.pin);
+      DP_LAUNCH_CHECK();
+    } else {
+      chebyshev<T>(c, L, b, x, true, o);
+      for (int s = 1; s < o.coarse_sweeps; ++s) chebyshev<T>(c, L, b, x, false, o);
+    }
+    return;
+  }
+  MGLevel& C = c.mg[l + 1];
+  chebyshev<T>(c, L, b, x, true, o);
+  // residual r = b - A x into L.r
+  T* r = (T*)L.r;
+  apply_level<T>(c, L, x, r);
+  k_sub<T><<<tpb(n), 256, 0, c.stream>>>(b, r, n);
+  const int64_t nc = 2 * C.g.nnod;
+  T* bc = (T*)C.b;
+  T* xc = (T*)C.x;
+  DP_CUDA(cudaMemsetAsync(bc, 0, sizeof(T) * nc, c.stream));
+  k_restrict<T><<<tpb(L.g.nnod), 256, 0, c.stream>>>(r, bc, (int)L.g.A(), (int)L.g.B(), C.g.ncr, (int)C.g.A(),
+                                                       (int)C.g.B(), L.g.pin);
+  k_mask_fixed<T><<<tpb(2 * C.g.B() + 1), 256, 0, c.stream>>>(bc, (int)C.g.A(), (int)C.g.B(), C.g.pin);
+  DP_LAUNCH_CHECK();
+  vcycle<T>(c, l + 1, bc, xc, o);
+  k_prolong_add<T><<<tpb(L.g.nnod), 256, 0, c.stream>>>(xc, x, (int)L.g.A(), (int)L.g.B(), C.g.ncr, (int)C.g.A(),
+                                                          (int)C.g.B(), L.g.pin);
+  DP_LAUNCH_CHECK();
+  chebyshev<T>(c, L, b, x, false, o);
+}
+
+void mg_apply(Ctx& c, const double* b, double* x, const MGOptions& o) { vcycle<double>(c, 0, b, x, o); }
+void mg_apply_f(Ctx& c, const float* b, float* x, const MGOptions& o) { vcycle<float>(c, 0, b, x, o); }
+
+}  // namespace dp

@@ -1,0 +1,227 @@
+// Operator applies, reductions and vector kernels.
+//
+// A-apply (K x): element-by-element from the stored packed polar element
+// matrices (the element blocks of StokesSolver.jl:688-810 after the rotation
+// of :192-201), gathering the 12 element DOFs through the analytic lattice
+// connectivity and scatter-adding the 12 results.
+// G / G^T applies: element-local 12x3 blocks (StokesSolver.jl:812-823), as the
+// SpMVs GG*q and GG'*z of IterativeSolvers.jl:142,144.
+// Dots: deterministic two-level reduction (warp shuffles -> block -> fixed-order
+// sum of the per-block partials by the last block), the role of mydot /
+// mynorm / vmean in Algebra.jl:104-113 and IterativeSolvers.jl:179-186.
+#include "kernels.cuh"
+#include "reduce.cuh"
+
+namespace dp {
+
+// ---- element-by-element K apply -------------------------------------------
+template <typename Tm, typename Tv>
+__global__ void __launch_bounds__(128) k_apply_K(const Tm* __restrict__ K, const Tv* __restrict__ x,
+                                                 Tv* __restrict__ y, int nel, int ncr, int A, int B) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nel) return;
+  const int q = e >> 1, t = e & 1;
+  const int ir = q % ncr, it = q / ncr;
+  const int a0 = 2 * ir, b0 = 2 * it;
+  int nd[6];
+  {
+    int bb[6], aa[6];
+    if (t == 0) {
+      aa[0] = a0; aa[1] = a0; aa[2] = a0 + 2; aa[3] = a0; aa[4] = a0 + 1; aa[5] = a0 + 1;
+      bb[0] = b0; bb[1] = b0 + 2; bb[2] = b0; bb[3] = b0 + 1; bb[4] = b0 + 1; bb[5] = b0;
+    } else {
+      aa[0] = a0; aa[1] = a0 + 2; aa[2] = a0 + 2; aa[3] = a0 + 1; aa[4] = a0 + 2; aa[5] = a0 + 1;
+      bb[0] = b0 + 2; bb[1] = b0 + 2; bb[2] = b0; bb[3] = b0 + 2; bb[4] = b0 + 1; bb[5] = b0 + 1;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) nd[k] = aa[k] + A * (bb[k] >= B ? bb[k] - B : bb[k]);
+  }
+  Tv xe[12], ye[12];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    xe[2 * k] = x[2 * nd[k]];
+    xe[2 * k + 1] = x[2 * nd[k] + 1];
+    ye[2 * k] = 0;
+    ye[2 * k + 1] = 0;
+  }
+#pragma unroll
+  for (int C = 0; C < 12; ++C) {
+#pragma unroll
+    for (int R = C; R < 12; ++R) {
+      const Tv kv = (Tv)K[(size_t)packed_index12(R, C) * nel + e];
+      ye[R] += kv * xe[C];
+      if (R != C) ye[C] += kv * xe[R];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    atomicAdd(&y[2 * nd[k]], ye[2 * k]);
+    atomicAdd(&y[2 * nd[k] + 1], ye[2 * k + 1]);
+  }
+}
+
+template <typename Tm, typename Tv>
+void launch_apply_K(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
+  DP_CUDA(cudaMemsetAsync(y, 0, sizeof(Tv) * 2 * L.nnod, s));
+  k_apply_K<Tm, Tv><<<(int)div_up(L.nel, 128), 128, 0, s>>>(K, x, y, (int)L.nel, L.ncr, (int)L.A(), (int)L.B());
+  DP_LAUNCH_CHECK();
+}
+template void launch_apply_K<double, double>(const Level&, const double*, const double*, double*, cudaStream_t);
+template void launch_apply_K<float, float>(const Level&, const float*, const float*, float*, cudaStream_t);
+
+// ---- G / G^T ----------------------------------------------------------------
+__device__ inline void element_nodes_dev(int e, int ncr, int A, int B, int nd[6]) {
+  const int q = e >> 1, t = e & 1;
+  const int ir = q % ncr, it = q / ncr;
+  const int a0 = 2 * ir, b0 = 2 * it;
+  int aa[6], bb[6];
+  if (t == 0) {
+    aa[0] = a0; aa[1] = a0; aa[2] = a0 + 2; aa[3] = a0; aa[4] = a0 + 1; aa[5] = a0 + 1;
+    bb[0] = b0; bb[1] = b0 + 2; bb[2] = b0; bb[3] = b0 + 1; bb[4] = b0 + 1; bb[5] = b0;
+  } else {
+    aa[0] = a0; aa[1] = a0 + 2; aa[2] = a0 + 2; aa[3] = a0 + 1; aa[4] = a0 + 2; aa[5] = a0 + 1;
+    bb[0] = b0 + 2; bb[1] = b0 + 2; bb[2] = b0; bb[3] = b0 + 2; bb[4] = b0 + 1; bb[5] = b0 + 1;
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) nd[k] = aa[k] + A * (bb[k] >= B ? bb[k] - B : bb[k]);
+}
+
+__device__ inline void element_pdofs_dev(int e, int ncr, int nct, int pressure, int pd[3]) {
+  if (pressure == 1) {
+    pd[0] = 3 * e; pd[1] = 3 * e + 1; pd[2] = 3 * e + 2;
+    return;
+  }
+  const int q = e >> 1, t = e & 1;
+  const int ir = q % ncr, it = q / ncr;
+  const int nr = ncr + 1;
+  const int it1 = (it + 1 == nct) ? 0 : it + 1;
+  const int v1 = ir + nr * it, v2 = ir + nr * it1, v3 = ir + 1 + nr * it1, v4 = ir + 1 + nr * it;
+  if (t == 0) { pd[0] = v1; pd[1] = v2; pd[2] = v4; }
+  else        { pd[0] = v2; pd[1] = v3; pd[2] = v4; }
+}
+
+__global__ void k_apply_G(const double* __restrict__ G, const double* __restrict__ p, double* __restrict__ y,
+                          int nel, int ncr, int nct, int A, int B, int pressure) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nel) return;
+  int nd[6], pd[3];
+  element_nodes_dev(e, ncr, A, B, nd);
+  element_pdofs_dev(e, ncr, nct, pressure, pd);
+  const double p0 = p[pd[0]], p1 = p[pd[1]], p2 = p[pd[2]];
+#pragma unroll
+  for (int d = 0; d < 12; ++d) {
+    const double v = G[(size_t)d * nel + e] * p0 + G[(size_t)(12 + d) * nel + e] * p1 +
+                     G[(size_t)(24 + d) * nel + e] * p2;
+    atomicAdd(&y[2 * nd[d >> 1] + (d & 1)], v);
+  }
+}
+
+__global__ void k_apply_GT(const double* __restrict__ G, const double* __restrict__ x, double* __restrict__ p,
+                           int nel, int ncr, int nct, int A, int B, int pressure) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nel) return;
+  int nd[6], pd[3];
+  element_nodes_dev(e, ncr, A, B, nd);
+  element_pdofs_dev(e, ncr, nct, pressure, pd);
+  double xe[12];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) { xe[2 * k] = x[2 * nd[k]]; xe[2 * k + 1] = x[2 * nd[k] + 1]; }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    double s = 0.0;
+#pragma unroll
+    for (int d = 0; d < 12; ++d) s += G[(size_t)(i * 12 + d) * nel + e] * xe[d];
+    if (pressure == 1) p[pd[i]] = s;
+    else atomicAdd(&p[pd[i]], s);
+  }
+}
+
+void launch_apply_G(Ctx& c, const double* p, double* y) {
+  const Level& L = c.fine;
+  DP_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * 2 * L.nnod, c.stream));
+  k_apply_G<<<(int)div_up(L.nel, 128), 128, 0, c.stream>>>(c.Gp, p, y, (int)L.nel, L.ncr, L.nct, (int)L.A(),
+                                                           (int)L.B(), c.mesh.pressure);
+  DP_LAUNCH_CHECK();
+}
+
+void launch_apply_GT(Ctx& c, const double* x, double* p) {
+  const Level& L = c.fine;
+  if (c.mesh.pressure == 0) DP_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * c.mesh.npres, c.stream));
+  k_apply_GT<<<(int)div_up(L.nel, 128), 128, 0, c.stream>>>(c.Gp, x, p, (int)L.nel, L.ncr, L.nct, (int)L.A(),
+                                                            (int)L.B(), c.mesh.pressure);
+  DP_LAUNCH_CHECK();
+}
+
+// ---- deterministic reductions ---------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_dot(const T* __restrict__ a, const T* __restrict__ b, int64_t n,
+                                                     double* partial, unsigned int* counter, double* out) {
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads)
+    s += (double)a[i] * (double)b[i];
+  double v[1] = {s};
+  double* o[1] = {out};
+  grid_finish<1>(v, partial, counter, o);
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_sum(const double* __restrict__ a, int64_t n, double* partial,
+                                                     unsigned int* counter, double* out) {
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads)
+    s += a[i];
+  double v[1] = {s};
+  double* o[1] = {out};
+  grid_finish<1>(v, partial, counter, o);
+}
+
+static int red_blocks(int64_t n) { return red_grid(n); }
+
+void launch_dot(Ctx& c, const double* a, const double* b, int64_t n, int slot) {
+  k_dot<double><<<red_blocks(n), kRedThreads, 0, c.stream>>>(a, b, n, c.partial, c.counter, c.scal + slot);
+  DP_LAUNCH_CHECK();
+}
+void launch_dot_f(Ctx& c, const float* a, const float* b, int64_t n, int slot) {
+  k_dot<float><<<red_blocks(n), kRedThreads, 0, c.stream>>>(a, b, n, c.partial, c.counter, c.scal + slot);
+  DP_LAUNCH_CHECK();
+}
+void launch_sum(Ctx& c, const double* a, int64_t n, int slot) {
+  k_sum<<<red_blocks(n), kRedThreads, 0, c.stream>>>(a, n, c.partial, c.counter, c.scal + slot);
+  DP_LAUNCH_CHECK();
+}
+
+// ---- permutations between reference numbering and the lattice -------------
+__global__ void k_gather_ref2lat(const int64_t* __restrict__ ref2lat, const double* __restrict__ ref,
+                                 double* __restrict__ lat, int64_t nnod, int comps) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nnod) return;
+  const int64_t l = ref2lat[n];
+  for (int c = 0; c < comps; ++c) lat[comps * l + c] = ref[comps * n + c];
+}
+__global__ void k_scatter_lat2ref(const int64_t* __restrict__ ref2lat, const double* __restrict__ lat,
+                                  double* __restrict__ ref, int64_t nnod, int comps) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nnod) return;
+  const int64_t l = ref2lat[n];
+  for (int c = 0; c < comps; ++c) ref[comps * n + c] = lat[comps * l + c];
+}
+void launch_gather_ref2lat(Ctx& c, const double* ref, double* lat, int comps) {
+  const int64_t n = c.fine.nnod;
+  k_gather_ref2lat<<<(int)div_up(n, 256), 256, 0, c.stream>>>(c.ref2lat, ref, lat, n, comps);
+  DP_LAUNCH_CHECK();
+}
+void launch_scatter_lat2ref(Ctx& c, const double* lat, double* ref, int comps) {
+  const int64_t n = c.fine.nnod;
+  k_scatter_lat2ref<<<(int)div_up(n, 256), 256, 0, c.stream>>>(c.ref2lat, lat, ref, n, comps);
+  DP_LAUNCH_CHECK();
+}
+
+__global__ void k_pc_invert(double* pc, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) pc[i] = 1.0 / pc[i];
+}
+void launch_pc_invert(Ctx& c, double* pc, int64_t n) {
+  k_pc_invert<<<(int)div_up(n, 256), 256, 0, c.stream>>>(pc, n);
+  DP_LAUNCH_CHECK();
+}
+
+}  // namespace dp

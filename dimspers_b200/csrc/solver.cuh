@@ -1,0 +1,49 @@
+// Solver configuration and work-vector layout.
+#pragma once
+#include "ctx.cuh"
+#include "mg.cuh"
+
+namespace dp {
+
+struct SolveCfg {
+  double rtol = 1e-8;       // outer (IterativeSolvers.jl:95)
+  int itmax = 200;          // outer (:96)
+  int itmin = 10;           // outer (:97)
+  int precision = 0;        // 0 FP64, 1 FP32-refined
+  int inner_pc = 0;         // 0 multigrid, 1 Jacobi
+  double inner_rtol = 1e-10;
+  double inner_rtol32 = 1e-5;
+  int inner_itmax = 500;
+  int max_refine = 6;
+  int remove_rotation = 1;
+  int use_guess = 0;
+  int verbose = 0;
+  MGOptions mg;
+};
+
+struct InnerStats {
+  int64_t its = 0;
+  double last_relres = 0.0;
+};
+
+struct SolveResult {
+  int status = 0;
+  int iterations = 0;
+  int64_t inner_its = 0;
+  double relres = 0.0, r0 = 0.0, omega = 0.0, div_residual = 0.0, mom_residual = 0.0;
+};
+
+// indices into Ctx::work
+enum Work {
+  W_R = 0, W_RLAST, W_D, W_Q, W_SQ,                 // pressure-sized (FP64)
+  W_Y, W_Z, W_RHS, W_IN_R, W_IN_Z, W_IN_P, W_IN_AP, W_RES,   // velocity-sized (FP64)
+  W_F_B, W_F_X, W_F_R, W_F_Z, W_F_P, W_F_AP,        // velocity-sized (FP32)
+  W_U, W_P, W_UC,                                   // solution staging (FP64)
+  W_COUNT
+};
+
+int inner_solve(Ctx& c, const double* y, double* z, const SolveCfg& cfg, InnerStats& st);
+int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& res);
+void to_cartesian(Ctx& c, const double* U, double* Uc);
+
+}  // namespace dp

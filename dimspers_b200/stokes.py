@@ -1,0 +1,262 @@
+"""Host-side mirror of the reference's Stokes interface over the C ABI.
+
+Reference call being replaced (src/Stokes/StokesSolver.jl:7-54)::
+
+    Ucartesian, Upolar, U, Ucart, P, to = solveStokes(U, P, T, gr, Ucartesian, Upolar, g, rho,
+        eta, C, epsII, coordinates, RotationMatrices, PhaseID, UBC, KKidx, GGidx, MMidx, to;
+        solver=:suitesparse)
+
+Here ``StokesContext`` owns the device side of one annulus mesh (mesh,
+lattice permutation, element blocks, multigrid hierarchy).  ``solve_stokes``
+is the one-call equivalent of ``solveStokes``: assembly
+(assembly_stokes_cylindric), rotation/BCs (_prepare_matrices, _apply_bcs),
+the Schur PCG (StokesPcCG) and the rigid-rotation removal (updatevelocity2).
+Arrays use the reference layouts (1-based indices are converted at the ABI):
+U interleaved [u_theta, u_r] per node, P continuous (vertex) or
+discontinuous (3 per element), eta.ip (nel, 7), tensor fields (nel, 7).
+"""
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import (DP_MEM_DEVICE, DP_MEM_HOST, DP_PRESSURE_CONTINUOUS, DP_PRESSURE_DISCONTINUOUS, MeshDesc,
+                   SolveOpts, SolveReport, check, lib)
+
+R_IN, R_OUT = 1.22, 2.22
+PRESSURE = {"continuous": DP_PRESSURE_CONTINUOUS, "discontinuous": DP_PRESSURE_DISCONTINUOUS}
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def mesh_desc(nr_cells, ntheta_cells, pressure="discontinuous", device=0, pin_rotation=True,
+              r_in=R_IN, r_out=R_OUT):
+    return MeshDesc(int(nr_cells), int(ntheta_cells), float(r_in), float(r_out), PRESSURE[pressure],
+                    int(device), 1 if pin_rotation else 0)
+
+
+@dataclass
+class Mesh:
+    """Host copy of the split-1 annulus mesh in the reference numbering
+    (Grid_split1, mesher.jl:152-233; color_mesh, coloring.jl:5-64)."""
+    nr_cells: int
+    ntheta_cells: int
+    pressure: str
+    pin_rotation: bool
+    e2n: np.ndarray      # (6, nel) 0-based
+    theta: np.ndarray    # (nnod,)
+    r: np.ndarray
+    colors: np.ndarray   # (nel,) 1-based
+    ncolors: int
+    omega: np.ndarray    # fixed DOFs, 0-based
+    nel: int
+    nnod: int
+    npres: int
+
+    @property
+    def th_el(self):
+        return self.element_coordinates()[0]
+
+    @property
+    def r_el(self):
+        return self.element_coordinates()[1]
+
+    def element_coordinates(self):
+        """Seam-fixed vertex coordinates (elementcoordinate + fixangles!,
+        Utilities.jl:30-61)."""
+        if not hasattr(self, "_elc"):
+            th = self.theta[self.e2n[:3]].copy()
+            r = self.r[self.e2n[:3]].copy()
+            a = (np.abs(th[0] - th[1]) + np.abs(th[1] - th[2]) + np.abs(th[2] - th[0])) > np.pi
+            th = np.where(a[None, :] & (th < np.pi), th + 2 * np.pi, th)
+            object.__setattr__(self, "_elc", (th, r))
+        return self._elc
+
+    @property
+    def ifree(self):
+        m = np.ones(2 * self.nnod, dtype=bool)
+        m[self.omega] = False
+        return np.flatnonzero(m)
+
+
+def build_mesh(nr_cells, ntheta_cells, pressure="discontinuous", pin_rotation=True, colors=True):
+    d = mesh_desc(nr_cells, ntheta_cells, pressure, pin_rotation=pin_rotation)
+    L = lib()
+    nel, nnod, npres, nfix = (C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64())
+    check(L.dp_mesh_sizes(C.byref(d), C.byref(nel), C.byref(nnod), C.byref(npres), C.byref(nfix)))
+    e2n = np.empty((nel.value, 6), dtype=np.int64)
+    th = np.empty(nnod.value)
+    r = np.empty(nnod.value)
+    col = np.empty(nel.value, dtype=np.int32)
+    ncol = C.c_int32(0)
+    check(L.dp_mesh_build(C.byref(d), e2n.ctypes.data_as(_lib._I64), th.ctypes.data_as(_lib._D),
+                          r.ctypes.data_as(_lib._D), col.ctypes.data_as(_lib._I32) if colors else None,
+                          C.byref(ncol) if colors else None))
+    om = np.empty(nfix.value, dtype=np.int64)
+    nom = C.c_int64(0)
+    check(L.dp_mesh_free_slip(C.byref(d), om.ctypes.data_as(_lib._I64), C.byref(nom)))
+    return Mesh(int(nr_cells), int(ntheta_cells), pressure, bool(pin_rotation), e2n.T - 1, th, r, col,
+                int(ncol.value), om[:nom.value] - 1, int(nel.value), int(nnod.value), int(npres.value))
+
+
+def default_opts(**kw):
+    o = SolveOpts()
+    lib().dp_default_opts(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    return o
+
+
+class StokesContext:
+    """Device context for one annulus mesh (dp_ctx)."""
+
+    def __init__(self, nr_cells, ntheta_cells, pressure="discontinuous", device=0, pin_rotation=True):
+        self.desc = mesh_desc(nr_cells, ntheta_cells, pressure, device, pin_rotation)
+        self.h = C.c_void_p()
+        check(lib().dp_ctx_create(C.byref(self.desc), C.byref(self.h)))
+        self.mesh = build_mesh(nr_cells, ntheta_cells, pressure, pin_rotation, colors=False)
+        self.nel, self.nnod, self.npres = self.mesh.nel, self.mesh.nnod, self.mesh.npres
+
+    def close(self):
+        if self.h:
+            lib().dp_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def stream(self):
+        return lib().dp_ctx_stream(self.h)
+
+    def _chk(self, st):
+        check(st, self.h)
+
+    def connectivity(self):
+        e2n = np.empty((self.nel, 6), dtype=np.int64)
+        col = np.empty(self.nel, dtype=np.int32)
+        self._chk(lib().dp_get_connectivity(self.h, e2n.ctypes.data_as(_lib._I64), col.ctypes.data_as(_lib._I32)))
+        return e2n.T - 1, col
+
+    # ---- material -----------------------------------------------------------
+    def set_material(self, eta_ip, rho, g, C6=None):
+        """eta_ip (nel, >=6) Fortran-or-C layout handled; C6 six (nel, >=6)."""
+        eta = np.asfortranarray(eta_ip, dtype=np.float64)
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        fields = None
+        keep = [eta, rho]
+        ldc = 0
+        if C6 is not None:
+            cs = [np.asfortranarray(c, dtype=np.float64) for c in C6]
+            keep += cs
+            fields = (C.c_void_p * 6)(*[c.ctypes.data for c in cs])
+            ldc = cs[0].shape[0]
+        self._chk(lib().dp_set_material(self.h, _ptr(eta), eta.shape[0], fields, ldc, _ptr(rho), float(g),
+                                        DP_MEM_HOST))
+
+    def set_material_ti(self, eta_ip, rho, g, delta, dir_x, dir_y):
+        eta = np.asfortranarray(eta_ip, dtype=np.float64)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (delta, dir_x, dir_y, rho)]
+        self._chk(lib().dp_set_material_ti(self.h, _ptr(eta), eta.shape[0], _ptr(arrs[0]), _ptr(arrs[1]),
+                                           _ptr(arrs[2]), _ptr(arrs[3]), float(g), DP_MEM_HOST))
+
+    def fse_director(self, F):
+        """F: (nel, 2, 2) per-element deformation gradient -> (dir_x, dir_y)."""
+        Fj = np.ascontiguousarray(np.asarray(F, dtype=np.float64).transpose(0, 2, 1).reshape(self.nel, 4))
+        dx = np.empty(self.nel)
+        dy = np.empty(self.nel)
+        self._chk(lib().dp_fse_director(self.h, _ptr(Fj), _ptr(dx), _ptr(dy), DP_MEM_HOST))
+        return dx, dy
+
+    # ---- assembly & operators -------------------------------------------------
+    def assemble(self, precision=0):
+        self._chk(lib().dp_assemble(self.h, int(precision)))
+
+    def element_matrices(self):
+        Ke = np.empty((self.nel, 78))
+        Ge = np.empty((self.nel, 36))
+        Me = np.empty((self.nel, 6))
+        Fb = np.empty((self.nel, 12))
+        self._chk(lib().dp_get_element_matrices(self.h, _ptr(Ke), _ptr(Ge), _ptr(Me), _ptr(Fb)))
+        return Ke.T, Ge.T, Me.T, Fb.T
+
+    def apply_K(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(2 * self.nnod)
+        self._chk(lib().dp_apply_K(self.h, _ptr(x), _ptr(y), DP_MEM_HOST))
+        return y
+
+    def apply_G(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        y = np.empty(2 * self.nnod)
+        self._chk(lib().dp_apply_G(self.h, _ptr(p), _ptr(y), DP_MEM_HOST))
+        return y
+
+    def apply_GT(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        p = np.empty(self.npres)
+        self._chk(lib().dp_apply_GT(self.h, _ptr(x), _ptr(p), DP_MEM_HOST))
+        return p
+
+    def rhs(self):
+        F = np.empty(2 * self.nnod)
+        pc = np.empty(self.npres)
+        self._chk(lib().dp_get_rhs(self.h, _ptr(F), _ptr(pc)))
+        return F, pc
+
+    # ---- solve ----------------------------------------------------------------
+    def solve(self, P0=None, want_cart=True, raise_on_status=True, **opts):
+        """StokesPcCG + updatevelocity2 -> (U, P, Ucart, report dict)."""
+        o = default_opts(**opts)
+        U = np.zeros(2 * self.nnod)
+        P = np.zeros(self.npres) if P0 is None else np.array(P0, dtype=np.float64)
+        if P0 is not None:
+            o.use_guess = 1
+        Uc = np.zeros(2 * self.nnod) if want_cart else None
+        rep = SolveReport()
+        st = lib().dp_solve(self.h, _ptr(U), _ptr(P), _ptr(Uc), C.byref(o), C.byref(rep), DP_MEM_HOST)
+        if st != 0 and (raise_on_status or st >= 3):
+            self._chk(st)
+        return U, P, Uc, rep.as_dict()
+
+    def solve_device(self, U_ptr, P_ptr, Uc_ptr=None, **opts):
+        """Same as solve() on device pointers (ints); returns the report dict."""
+        o = default_opts(**opts)
+        rep = SolveReport()
+        st = lib().dp_solve(self.h, C.c_void_p(U_ptr), C.c_void_p(P_ptr),
+                            C.c_void_p(Uc_ptr) if Uc_ptr else None, C.byref(o), C.byref(rep), DP_MEM_DEVICE)
+        if st >= 3:
+            self._chk(st)
+        return rep.as_dict()
+
+    def set_material_device(self, eta_ptr, ld_eta, rho_ptr, g, C6_ptrs=None, ld_C=0):
+        fields = (C.c_void_p * 6)(*C6_ptrs) if C6_ptrs is not None else None
+        self._chk(lib().dp_set_material(self.h, C.c_void_p(eta_ptr), int(ld_eta), fields, int(ld_C),
+                                        C.c_void_p(rho_ptr), float(g), DP_MEM_DEVICE))
+
+    def set_material_ti_device(self, eta_ptr, ld_eta, rho_ptr, g, delta_ptr, dx_ptr, dy_ptr):
+        self._chk(lib().dp_set_material_ti(self.h, C.c_void_p(eta_ptr), int(ld_eta), C.c_void_p(delta_ptr),
+                                           C.c_void_p(dx_ptr), C.c_void_p(dy_ptr), C.c_void_p(rho_ptr), float(g),
+                                           DP_MEM_DEVICE))
+
+
+def solve_stokes(ctx, eta_ip, rho, g, C6=None, precision=0, P0=None, **opts):
+    """solveStokes (StokesSolver.jl:7-54) on a StokesContext: set material,
+    assemble, Schur PCG, rigid-rotation removal.  Returns (U, P, Ucart, report)."""
+    ctx.set_material(eta_ip, rho, g, C6)
+    ctx.assemble(precision)
+    return ctx.solve(P0=P0, precision=precision, **opts)

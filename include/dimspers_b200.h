@@ -1,0 +1,172 @@
+/*
+ * dimspers_b200 -- C ABI of the B200 Stokes hot path (P2-P1 annulus assembly
+ * and Schur-complement PCG) of DimsPers / Persephone.
+ *
+ * Every entry point returns a status code (dp_status) and never exits or
+ * aborts.  Host arrays are borrowed for the duration of a call.  Device
+ * buffers are owned by the context.  Index arrays crossing the ABI are
+ * 1-based and column-major as Julia stores them.  One context per host
+ * thread; calls are synchronous to the caller (stream-ordered inside).
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   solveStokes                src/Stokes/StokesSolver.jl:7-54
+ *   assembly_stokes_cylindric  src/Stokes/StokesSolver.jl:247-404
+ *   _prepare_matrices          src/Stokes/StokesSolver.jl:192-201
+ *   _apply_bcs                 src/Stokes/StokesSolver.jl:186-190
+ *   StokesPcCG                 src/IterativeSolvers.jl:94-168
+ *   updatevelocity2            src/Stokes/StokesSolver.jl:170-184
+ *   Grid_split1 / color_mesh   src/Grid/mesher.jl:152-233, src/Grid/coloring.jl:5-64
+ */
+#ifndef DIMSPERS_B200_H
+#define DIMSPERS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  DP_OK = 0,
+  DP_NOT_CONVERGED = 1,  /* outer itmax reached (the reference returns silently) */
+  DP_BREAKDOWN = 2,      /* q.Sq <= 0 or a non-finite scalar in the PCG        */
+  DP_BAD_ARG = 3,
+  DP_CUDA_ERROR = 4,
+  DP_DEVICE_TIMEOUT = 5
+} dp_status;
+
+typedef enum { DP_PRESSURE_CONTINUOUS = 0, DP_PRESSURE_DISCONTINUOUS = 1 } dp_pressure_space;
+typedef enum { DP_PREC_FP64 = 0, DP_PREC_FP32_REFINED = 1 } dp_precision;
+typedef enum { DP_MEM_HOST = 0, DP_MEM_DEVICE = 1 } dp_memory;
+typedef enum { DP_INNER_MG = 0, DP_INNER_JACOBI = 1 } dp_inner_pc;
+
+/* Mesh description.  Cells, not nodes: the reference's init_grid/Grid_split1
+ * take node counts (nr = cells + 1, ntheta = cells). */
+typedef struct {
+  int32_t nr_cells;        /* radial cells (>= 1)                              */
+  int32_t ntheta_cells;    /* angular cells (>= 3)                             */
+  double r_in, r_out;      /* radii (1.22, 2.22 in the reference)              */
+  int32_t pressure_space;  /* dp_pressure_space                               */
+  int32_t device;          /* CUDA device ordinal                             */
+  int32_t pin_rotation;    /* 1: also fix u_theta of the outer-wall node at
+                              theta = 0 (free_slip(nr, ids),
+                              boundary_conditions.jl:180-194), which removes the
+                              rigid-rotation near-null mode of K; 0: the plain
+                              free_slip(ids) of MAIN.jl                         */
+} dp_mesh_desc;
+
+typedef struct {
+  double rtol;             /* outer relative tolerance (reference: 1e-8)      */
+  int32_t itmax;           /* outer iteration cap (reference: 200)            */
+  int32_t itmin;           /* outer minimum iterations (reference: 10)        */
+  int32_t precision;       /* dp_precision                                    */
+  int32_t inner_pc;        /* dp_inner_pc                                     */
+  double inner_rtol;       /* inner K-solve relative tolerance                */
+  int32_t inner_itmax;     /* inner iteration cap                             */
+  int32_t remove_rotation; /* apply updatevelocity2's rigid-rotation removal  */
+  int32_t use_guess;       /* 1: start from the P passed in (else P = 0)      */
+  int32_t verbose;
+  int32_t cheb_degree;     /* Chebyshev smoothing steps per level             */
+  double inner_rtol32;     /* FP32 inner tolerance per refinement step        */
+  int32_t max_refine;      /* FP32-refined: refinement steps per inner solve  */
+} dp_solve_opts;
+
+typedef struct {
+  int32_t status;
+  int32_t iterations;          /* outer (Schur) iterations                    */
+  int64_t inner_iterations;    /* total inner K-solve iterations              */
+  double relres;               /* final outer ||r|| / ||r0|| (reference measure) */
+  double r0;                   /* ||r0||                                       */
+  double omega;                /* removed rigid angular velocity              */
+  double div_residual;         /* ||G^T U|| / ||G^T U0||                       */
+  double mom_residual;         /* ||K U - F - G P|| / ||F|| on free DOFs       */
+  double t_assemble_ms, t_setup_ms, t_solve_ms;
+  int32_t fallback_used;       /* learned guess rejected -> zero guess        */
+  int32_t mg_levels;
+} dp_solve_report;
+
+typedef struct dp_ctx dp_ctx;
+
+/* ---- host-only queries (no GPU needed) --------------------------------- */
+
+/* Sizes of the split-1 P2 mesh (mesher.jl:152-233). */
+int dp_mesh_sizes(const dp_mesh_desc* desc, int64_t* nel, int64_t* nnod,
+                  int64_t* npres, int64_t* nfixed);
+
+/* Build the mesh on the host in the reference's numbering:
+ *   e2n     6 x nel, column-major, 1-based  (gr.e2n, mesher.jl:202-204)
+ *   theta,r nnod                            (gr.theta, gr.r incl. midpoints)
+ *   colors  nel, 1-based greedy colours     (color_mesh, coloring.jl:5-64)
+ *   ncolors number of colours
+ * Any output pointer may be NULL. */
+int dp_mesh_build(const dp_mesh_desc* desc, int64_t* e2n, double* theta, double* r,
+                  int32_t* colors, int32_t* ncolors);
+
+/* Free-slip constraint set (boundary_conditions.jl:15-37): Omega (1-based
+ * DOFs 2*node of wall nodes, top then bottom) and its count. */
+int dp_mesh_free_slip(const dp_mesh_desc* desc, int64_t* omega, int64_t* nomega);
+
+const char* dp_status_string(int status);
+
+/* ---- context ------------------------------------------------------------ */
+
+int dp_ctx_create(const dp_mesh_desc* desc, dp_ctx** out);
+void dp_ctx_destroy(dp_ctx* ctx);
+const char* dp_last_error(const dp_ctx* ctx);
+/* cudaStream_t the context launches on (as void*). */
+void* dp_ctx_stream(dp_ctx* ctx);
+int dp_get_connectivity(dp_ctx* ctx, int64_t* e2n, int32_t* colors);
+
+/* Material inputs in the reference layouts:
+ *   eta_ip   nel x ld columns, element-fastest (eta.ip; IPs 1..6 read)
+ *   C6       NULL (isotropic) or 6 pointers in StiffnessTensor order
+ *            (C11, C33, C55, C13, C15, C35), each nel x ld_C element-fastest
+ *   rho_node nnod nodal density (vertices enter the body force)
+ *   g        gravity factor (body force g*rho*r_hat)
+ * mem = dp_memory of every pointer. */
+int dp_set_material(dp_ctx* ctx, const double* eta_ip, int64_t ld_eta,
+                    const double* const* C6, int64_t ld_C, const double* rho_node,
+                    double g, int32_t mem);
+
+/* Transversely isotropic material: per-element delta (weak-plane shear
+ * viscosity eta/delta) and director (dir_x, dir_y); the tensor is the frame
+ * tensor a = c = 4/3, h = -2/3, e = 1/delta rotated on the device as in
+ * directRotation2D (anisotropy.jl:503-536). */
+int dp_set_material_ti(dp_ctx* ctx, const double* eta_ip, int64_t ld_eta,
+                       const double* delta, const double* dir_x, const double* dir_y,
+                       const double* rho_node, double g, int32_t mem);
+
+/* Director = major eigenvector of F F^T per element (FSE.jl:143-161).
+ * F is 4 x nel column-major (F11, F21, F12, F22 as a Julia 2x2 per element). */
+int dp_fse_director(dp_ctx* ctx, const double* F, double* dir_x, double* dir_y, int32_t mem);
+
+/* Element assembly + rotation + BC mask on the device (precision: dp_precision). */
+int dp_assemble(dp_ctx* ctx, int32_t precision);
+
+/* Copy the un-rotated Cartesian element blocks in the reference layouts
+ * (K_all 78 x nel, G_all 36 x nel, M_all 6 x nel, Fb_all 12 x nel, column-major).
+ * Any pointer may be NULL. */
+int dp_get_element_matrices(dp_ctx* ctx, double* Ke, double* Ge, double* Me, double* Fb);
+
+/* Full solve: StokesPcCG + optional rigid-rotation removal.  U (2*nnod,
+ * interleaved [u_theta, u_r] per node, reference numbering) and P (npres)
+ * are overwritten; Ucart (2*nnod, may be NULL) receives TT*U. */
+int dp_solve(dp_ctx* ctx, double* U, double* P, double* Ucart, const dp_solve_opts* opts,
+             dp_solve_report* report, int32_t mem);
+
+/* Operator applies for testing, on polar (rotated) DOFs in reference numbering:
+ * y = K x (free DOFs, fixed rows zero), yG = G p, pG = G^T x. */
+int dp_apply_K(dp_ctx* ctx, const double* x, double* y, int32_t mem);
+int dp_apply_G(dp_ctx* ctx, const double* p, double* y, int32_t mem);
+int dp_apply_GT(dp_ctx* ctx, const double* x, double* p, int32_t mem);
+/* Assembled right-hand side (polar, reference numbering) and lumped pressure
+ * preconditioner 1/rowsum(M). */
+int dp_get_rhs(dp_ctx* ctx, double* F, double* pc);
+
+void dp_default_opts(dp_solve_opts* opts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
