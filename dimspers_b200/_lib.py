@@ -12,7 +12,7 @@ LIB_PATH = os.path.join(HERE, "libdimspers_b200.so")
 
 DP_OK, DP_NOT_CONVERGED, DP_BREAKDOWN, DP_BAD_ARG, DP_CUDA_ERROR, DP_DEVICE_TIMEOUT = range(6)
 DP_PRESSURE_CONTINUOUS, DP_PRESSURE_DISCONTINUOUS = 0, 1
-DP_PREC_FP64, DP_PREC_FP32_REFINED = 0, 1
+DP_PREC_FP64, DP_PREC_FP32_REFINED, DP_PREC_FP32_IR = 0, 1, 2
 DP_MEM_HOST, DP_MEM_DEVICE = 0, 1
 DP_INNER_MG, DP_INNER_JACOBI = 0, 1
 
@@ -28,7 +28,9 @@ class SolveOpts(C.Structure):
                 ("precision", C.c_int32), ("inner_pc", C.c_int32), ("inner_rtol", C.c_double),
                 ("inner_itmax", C.c_int32), ("remove_rotation", C.c_int32), ("use_guess", C.c_int32),
                 ("verbose", C.c_int32), ("cheb_degree", C.c_int32), ("inner_rtol32", C.c_double),
-                ("max_refine", C.c_int32)]
+                ("max_refine", C.c_int32), ("host_loop", C.c_int32), ("block_jacobi", C.c_int32),
+                ("cheb_lo", C.c_double), ("cheb_hi", C.c_double), ("inner_relax", C.c_double),
+                ("coarse_max", C.c_int32), ("schur_pc", C.c_int32)]
 
 
 class SolveReport(C.Structure):
@@ -36,7 +38,8 @@ class SolveReport(C.Structure):
                 ("relres", C.c_double), ("r0", C.c_double), ("omega", C.c_double),
                 ("div_residual", C.c_double), ("mom_residual", C.c_double),
                 ("t_assemble_ms", C.c_double), ("t_setup_ms", C.c_double), ("t_solve_ms", C.c_double),
-                ("fallback_used", C.c_int32), ("mg_levels", C.c_int32)]
+                ("fallback_used", C.c_int32), ("mg_levels", C.c_int32), ("kernel_launches", C.c_int64),
+                ("refinements", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -69,6 +72,7 @@ SIGNATURES = {
     "dp_apply_GT": (C.c_int, [_P, _P, _P, C.c_int32]),
     "dp_get_rhs": (C.c_int, [_P, _P, _P]),
     "dp_default_opts": (None, [C.POINTER(SolveOpts)]),
+    "dp_profile_kernel": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
 }
 
 _lib = None

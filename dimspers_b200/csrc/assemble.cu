@@ -90,6 +90,7 @@ struct AsmArgs {
   double* Gp;          // 36*nel
   double* F;           // 2*nnod, accumulated with atomics (zeroed by caller)
   double* pcsum;       // npres: disc -> 1/rowsum written; cont -> rowsum accumulated
+  double* Minv;        // 6*nel: inverse of the element mass block (discontinuous pressure)
   CartOut cart;
 };
 
@@ -304,6 +305,18 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs p) {
     const double row[3] = {m00 + m10 + m20, m10 + m11 + m21, m20 + m21 + m22};
     if (p.pressure == 1) {
       for (int i = 0; i < 3; ++i) p.pcsum[3 * (size_t)e + i] = 1.0 / row[i];
+      // exact inverse of the symmetric 3x3 element block M_e (the whole of M for
+      // discontinuous pressure), packed (00, 10, 20, 11, 21, 22)
+      const double c00 = m11 * m22 - m21 * m21, c10 = -(m10 * m22 - m21 * m20), c20 = m10 * m21 - m11 * m20;
+      const double c11 = m00 * m22 - m20 * m20, c21 = -(m00 * m21 - m10 * m20), c22 = m00 * m11 - m10 * m10;
+      const double det = m00 * c00 + m10 * c10 + m20 * c20;
+      const double id = 1.0 / det;
+      p.Minv[(size_t)0 * p.nel + e] = c00 * id;
+      p.Minv[(size_t)1 * p.nel + e] = c10 * id;
+      p.Minv[(size_t)2 * p.nel + e] = c20 * id;
+      p.Minv[(size_t)3 * p.nel + e] = c11 * id;
+      p.Minv[(size_t)4 * p.nel + e] = c21 * id;
+      p.Minv[(size_t)5 * p.nel + e] = c22 * id;
     } else {
       int64_t pd[3];
       element_pdofs_cont(e, p.ncr, p.nct, pd);
@@ -323,8 +336,8 @@ void launch_assemble(Ctx& c, int precision, const CartOut* cart) {
   a.theta_lat = c.theta_lat; a.r_lat = c.r_lat; a.rho_lat = c.rho_lat;
   a.eta = c.eta; a.C = c.C; a.g = c.g;
   a.K64 = c.K64;
-  a.K32 = precision == 1 ? c.K32 : nullptr;
-  a.Gp = c.Gp; a.F = c.F; a.pcsum = c.pc;
+  a.K32 = precision >= 1 ? c.K32 : nullptr;
+  a.Gp = c.Gp; a.F = c.F; a.pcsum = c.pc; a.Minv = c.Minv;
   if (cart) a.cart = *cart;
   const size_t smem = sizeof(double) * kAcc * kAsmThreads;
   static bool attr_set = false;
@@ -335,6 +348,7 @@ void launch_assemble(Ctx& c, int precision, const CartOut* cart) {
   DP_CUDA(cudaMemsetAsync(c.F, 0, sizeof(double) * 2 * L.nnod, c.stream));
   if (c.mesh.pressure == 0) DP_CUDA(cudaMemsetAsync(c.pc, 0, sizeof(double) * c.mesh.npres, c.stream));
   const int grid = (int)div_up(L.nel, kAsmThreads);
+  ++g_klaunch;
   k_assemble<<<grid, kAsmThreads, smem, c.stream>>>(a);
   DP_LAUNCH_CHECK();
   if (c.mesh.pressure == 0) launch_pc_invert(c, c.pc, c.mesh.npres);
@@ -350,6 +364,7 @@ __global__ void k_ti_fill(int nel, const double* delta, const double* dx, const 
 
 void launch_ti_tensor_fill(Ctx& c, const double* delta, const double* dx, const double* dy) {
   const int nel = (int)c.fine.nel;
+  ++g_klaunch;
   k_ti_fill<<<(int)div_up(nel, 256), 256, 0, c.stream>>>(nel, delta, dx, dy, c.C);
   DP_LAUNCH_CHECK();
 }
@@ -376,6 +391,7 @@ __global__ void k_fse_director(int64_t nel, const double* F, double* dxo, double
 }
 
 void launch_fse_director(Ctx& c, const double* F, double* dx, double* dy, int64_t nel) {
+  ++g_klaunch;
   k_fse_director<<<(int)div_up(nel, 256), 256, 0, c.stream>>>(nel, F, dx, dy);
   DP_LAUNCH_CHECK();
 }

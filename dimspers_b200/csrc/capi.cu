@@ -21,10 +21,16 @@ namespace dp {
 static thread_local std::string g_err;
 
 Ctx::~Ctx() {
+  graph_free(*this);
+  cudaFree(ctl);
+  cudaFreeHost(h_ctl);
+  for (cudaStream_t s : aux)
+    if (s) cudaStreamDestroy(s);
   mg_free(*this);
   cudaFree(theta_lat); cudaFree(r_lat); cudaFree(ref2lat);
   cudaFree(eta); cudaFree(C); cudaFree(rho_lat); cudaFree(rho_ref);
-  cudaFree(K64); cudaFree(K32); cudaFree(Gp); cudaFree(F); cudaFree(pc); cudaFree(Fscale);
+  cudaFree(K64); cudaFree(K32); cudaFree(Gp); cudaFree(F); cudaFree(pc); cudaFree(Minv); cudaFree(Fscale);
+  cudaFree(flush);
   cudaFree(scal); cudaFreeHost(h_scal); cudaFree(partial); cudaFree(counter);
   for (void* p : work) cudaFree(p);
   if (stream) cudaStreamDestroy(stream);
@@ -104,9 +110,18 @@ static SolveCfg make_cfg(const dp_solve_opts* o) {
   if (o->cheb_degree > 0) cfg.mg.cheb_degree = o->cheb_degree;
   if (o->inner_rtol32 > 0) cfg.inner_rtol32 = o->inner_rtol32;
   if (o->max_refine > 0) cfg.max_refine = o->max_refine;
+  cfg.host_loop = o->host_loop;
+  cfg.mg.block_jacobi = o->block_jacobi;
+  if (o->cheb_lo > 0) cfg.mg.cheb_lo = o->cheb_lo;
+  if (o->cheb_hi > 0) cfg.mg.cheb_hi = o->cheb_hi;
+  if (!(cfg.mg.cheb_lo < cfg.mg.cheb_hi)) throw BadArg("cheb_lo must be below cheb_hi");
   if (!(cfg.rtol > 0) || cfg.itmax < 1 || cfg.itmin < 0 || !(cfg.inner_rtol > 0) || cfg.inner_itmax < 1)
     throw BadArg("invalid solve options");
-  if (cfg.precision != 0 && cfg.precision != 1) throw BadArg("precision must be 0 or 1");
+  if (cfg.precision < 0 || cfg.precision > 2) throw BadArg("precision must be 0, 1 or 2");
+  cfg.inner_relax = o->inner_relax;
+  if (o->coarse_max > 0) cfg.mg.coarse_max = o->coarse_max;
+  cfg.schur_pc = o->schur_pc;
+  if (cfg.schur_pc != 0 && cfg.schur_pc != 1) throw BadArg("schur_pc must be 0 (lumped) or 1 (mass)");
   if (cfg.inner_pc != 0 && cfg.inner_pc != 1) throw BadArg("inner_pc must be 0 or 1");
   return cfg;
 }
@@ -138,6 +153,12 @@ void dp_default_opts(dp_solve_opts* o) {
   o->cheb_degree = 3;
   o->inner_rtol32 = 1e-5;
   o->max_refine = 6;
+  o->host_loop = 0;
+  o->block_jacobi = 1;
+  o->cheb_lo = 0.1;
+  o->cheb_hi = 1.1;
+  o->inner_relax = 0.0;
+  o->coarse_max = 1024;
 }
 
 const char* dp_status_string(int s) {
@@ -233,6 +254,7 @@ int dp_ctx_create(const dp_mesh_desc* d, dp_ctx** out) {
     dalloc(&c.Gp, kGe * nel);
     dalloc(&c.F, 2 * nn);
     dalloc(&c.pc, np);
+    dalloc(&c.Minv, 6 * nel);
     dalloc(&c.scal, 64);
     DP_CUDA(cudaMemset(c.scal, 0, sizeof(double) * 64));
     DP_CUDA(cudaMallocHost((void**)&c.h_scal, sizeof(double) * 64));
@@ -362,8 +384,8 @@ int dp_assemble(dp_ctx* h, int32_t precision) {
   return guarded(&c, [&] {
     DP_CUDA(cudaSetDevice(c.device));
     if (c.mat_kind == MAT_NONE) throw BadArg("material not set");
-    if (precision != 0 && precision != 1) throw BadArg("precision must be 0 or 1");
-    if (precision == 1 && !c.K32) dalloc(&c.K32, kKe * c.fine.nel);
+    if (precision < 0 || precision > 2) throw BadArg("precision must be 0, 1 or 2");
+    if (precision >= 1 && !c.K32) dalloc(&c.K32, kKe * c.fine.nel);
     launch_assemble(c, precision, nullptr);
     c.assembled = precision;
     c.mg_prec = c.mg.empty() ? -1 : c.mg_prec;  // hierarchy values are rebuilt on the next solve
@@ -405,10 +427,13 @@ int dp_solve(dp_ctx* h, double* U, double* P, double* Ucart, const dp_solve_opts
     if (!U || !P) throw BadArg("null U or P");
     if (c.assembled < 0) throw BadArg("dp_assemble must run before dp_solve");
     SolveCfg cfg = make_cfg(opts);
+    if (cfg.schur_pc == 1 && c.mesh.pressure != 1)
+      throw BadArg("schur_pc = 1 (element-block mass inverse) needs discontinuous pressure");
     const int64_t nn = c.fine.nnod, np = c.mesh.npres;
-    if (cfg.precision == 1 && c.assembled == 0) {
+    if (cfg.precision >= 1 && c.assembled == 0) {
       if (!c.K32) dalloc(&c.K32, kKe * c.fine.nel);
       const int64_t n = kKe * c.fine.nel;
+      ++g_klaunch;
       k_f64_to_f32<<<(int)div_up(n, 256), 256, 0, c.stream>>>(c.K64, c.K32, n);
       DP_LAUNCH_CHECK();
       c.assembled = 1;
@@ -418,7 +443,7 @@ int dp_solve(dp_ctx* h, double* U, double* P, double* Ucart, const dp_solve_opts
     DP_CUDA(cudaEventCreate(&e1));
     DP_CUDA(cudaEventCreate(&e2));
     DP_CUDA(cudaEventRecord(e0, c.stream));
-    mg_setup(c, cfg.precision, cfg.mg);
+    mg_setup(c, cfg.precision >= 1 ? 1 : 0, cfg.mg);
     DP_CUDA(cudaEventRecord(e1, c.stream));
     double* dU = (double*)c.work[W_U];
     double* dP = (double*)c.work[W_P];
@@ -427,7 +452,13 @@ int dp_solve(dp_ctx* h, double* U, double* P, double* Ucart, const dp_solve_opts
     }
     DP_CUDA(cudaMemsetAsync(dU, 0, sizeof(double) * 2 * nn, c.stream));
     SolveResult res;
-    schur_pcg(c, cfg, dU, dP, res);
+    if (cfg.host_loop) {
+      const int64_t k0 = g_klaunch;
+      schur_pcg(c, cfg, dU, dP, res);
+      res.launches = g_klaunch - k0;
+    } else {
+      schur_pcg_graph(c, cfg, dU, dP, res);
+    }
     // lattice -> reference numbering
     double* stage = (double*)c.work[W_UC];
     launch_scatter_lat2ref(c, dU, stage, 2);
@@ -458,6 +489,8 @@ int dp_solve(dp_ctx* h, double* U, double* P, double* Ucart, const dp_solve_opts
       rep->t_setup_ms = ms_setup;
       rep->t_solve_ms = ms_solve;
       rep->mg_levels = (int)c.mg.size();
+      rep->kernel_launches = res.launches;
+      rep->refinements = res.refinements;
     }
     if (res.status == 1) c.err = "outer iteration cap reached";
     if (res.status == 2) c.err = "breakdown: q.Sq <= 0 or non-finite scalar";
@@ -502,6 +535,64 @@ static int apply_common(dp_ctx* h, const double* in, double* out, int32_t mem, i
 int dp_apply_K(dp_ctx* h, const double* x, double* y, int32_t mem) { return apply_common(h, x, y, mem, 0); }
 int dp_apply_G(dp_ctx* h, const double* p, double* y, int32_t mem) { return apply_common(h, p, y, mem, 1); }
 int dp_apply_GT(dp_ctx* h, const double* x, double* p, int32_t mem) { return apply_common(h, x, p, mem, 2); }
+
+int dp_profile_kernel(dp_ctx* h, int32_t which, int32_t reps, int32_t flush_l2, double* ms) {
+  if (!h) return DP_BAD_ARG;
+  Ctx& c = h->c;
+  return guarded(&c, [&] {
+    DP_CUDA(cudaSetDevice(c.device));
+    if (c.assembled < 0) throw BadArg("dp_assemble must run first");
+    if (reps < 1 || !ms) throw BadArg("reps must be >= 1");
+    if (which == 0 && !c.K32) throw BadArg("no FP32 element matrices (assemble with precision 1)");
+    if (which == 2 && c.mg.empty()) throw BadArg("no multigrid hierarchy (run a solve first)");
+    const int64_t n = 2 * c.fine.nnod;
+    double* x64 = (double*)c.work[W_IN_P];
+    double* y64 = (double*)c.work[W_IN_AP];
+    float* x32 = (float*)c.work[W_F_P];
+    float* y32 = (float*)c.work[W_F_AP];
+    DP_CUDA(cudaMemsetAsync(x64, 0, sizeof(double) * n, c.stream));
+    DP_CUDA(cudaMemsetAsync(x32, 0, sizeof(float) * n, c.stream));
+    auto once = [&] {
+      if (which == 0) launch_apply_K<float, float>(c.fine, c.K32, x32, y32, c.stream);
+      else if (which == 1) launch_apply_K<double, double>(c.fine, c.K64, x64, y64, c.stream);
+      else if (c.mg_prec == 1) mg_apply_f(c, x32, y32, MGOptions());
+      else mg_apply(c, x64, y64, MGOptions());
+    };
+    once();
+    cudaEvent_t e0, e1;
+    DP_CUDA(cudaEventCreate(&e0));
+    DP_CUDA(cudaEventCreate(&e1));
+    double total = 0.0;
+    if (flush_l2) {
+      // cold L2: overwrite a buffer of twice the L2 size before every launch
+      // and time each launch on its own
+      const size_t fb = 256ull << 20;
+      if (!c.flush) DP_CUDA(cudaMalloc(&c.flush, fb));
+      for (int i = 0; i < reps; ++i) {
+        DP_CUDA(cudaMemsetAsync(c.flush, i & 0xff, fb, c.stream));
+        DP_CUDA(cudaEventRecord(e0, c.stream));
+        once();
+        DP_CUDA(cudaEventRecord(e1, c.stream));
+        DP_CUDA(cudaEventSynchronize(e1));
+        float t = 0;
+        DP_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        total += t;
+      }
+    } else {
+      DP_CUDA(cudaEventRecord(e0, c.stream));
+      for (int i = 0; i < reps; ++i) once();
+      DP_CUDA(cudaEventRecord(e1, c.stream));
+      DP_CUDA(cudaEventSynchronize(e1));
+      float t = 0;
+      DP_CUDA(cudaEventElapsedTime(&t, e0, e1));
+      total = t;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = total / reps;
+    return (int)DP_OK;
+  });
+}
 
 int dp_get_rhs(dp_ctx* h, double* F, double* pc) {
   if (!h) return DP_BAD_ARG;

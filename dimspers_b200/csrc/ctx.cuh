@@ -22,6 +22,10 @@
 
 namespace dp {
 
+// Kernels launched by this thread (every launch site increments it); used to
+// report the launches of a solve and, while capturing, the kernels per graph body.
+inline thread_local int64_t g_klaunch = 0;
+
 constexpr int kNip = 6;
 constexpr int kKe = 78;   // packed lower 12x12
 constexpr int kGe = 36;   // 12x3 column-major
@@ -49,9 +53,10 @@ struct MGLevel {
   Level g;
   double* K64 = nullptr;     // 78*nel packed polar, masked
   float* K32 = nullptr;
-  double* dinv64 = nullptr;  // 2*nnod inverse diagonal (0 on fixed DOFs)
+  double* dinv64 = nullptr;  // 3*nnod inverse of the 2x2 nodal diagonal blocks (i00, i01, i11)
   float* dinv32 = nullptr;
   double lmax = 0.0;         // estimate of lambda_max(D^-1 A)
+  double* cheb = nullptr;    // device: [1/theta, -, (c1, c2) per further step]
   // work vectors (precision of the hierarchy)
   void* x = nullptr;
   void* b = nullptr;
@@ -87,11 +92,15 @@ struct Ctx {
   double* Gp = nullptr;         // 36*nel
   double* F = nullptr;          // 2*nnod
   double* pc = nullptr;         // npres (1/rowsum M)
+  double* Minv = nullptr;       // 6*nel inverse element mass blocks (discontinuous pressure)
   double* Fscale = nullptr;
+  void* flush = nullptr;        // L2 flush buffer for cold kernel timings
 
   // multigrid hierarchy (level 0 = fine)
   std::vector<MGLevel> mg;
   int mg_prec = -1;             // 0 = fp64, 1 = fp32
+  int mg_degree = 3;            // Chebyshev steps in use
+  int64_t mg_coarse_max = -1;   // coarse_max the hierarchy was built for
   double* coarse_chol = nullptr;// dense Cholesky factor of the coarsest level
   int64_t coarse_n = 0;
   int64_t* coarse_map = nullptr;// coarsest DOF -> dense index (-1 fixed)
@@ -102,6 +111,19 @@ struct Ctx {
   double* partial = nullptr;    // reduction partials
   unsigned int* counter = nullptr;
   std::vector<void*> work;      // solver vectors
+
+  // graph-captured solve (graph.cu)
+  void* ctl = nullptr;          // device control block (DevCtl)
+  void* h_ctl = nullptr;        // pinned host mirror
+  cudaStream_t aux[3] = {nullptr, nullptr, nullptr};  // capture streams of nested loop bodies
+  void* graph = nullptr;        // cudaGraph_t
+  void* gexec = nullptr;        // cudaGraphExec_t
+  int64_t gkey = -1;
+  const void* gU = nullptr;
+  const void* gP = nullptr;
+  int64_t gk_main = 0;          // kernel nodes outside loop bodies
+  int64_t cap_nested = 0;       // kernels captured inside nested bodies (capture bookkeeping)
+  int64_t gk_body[4] = {0, 0, 0, 0};  // kernel nodes per body execution (outer, pcg64, pcg32, refinement)
 
   ~Ctx();
 };

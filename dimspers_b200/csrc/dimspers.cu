@@ -5,4 +5,5 @@
 #include "ops.cu"
 #include "mg.cu"
 #include "solver.cu"
+#include "graph.cu"
 #include "capi.cu"

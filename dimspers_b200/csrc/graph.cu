@@ -1,0 +1,503 @@
+// The whole Stokes solve as one CUDA graph with device-side control flow.
+//
+// StokesPcCG (IterativeSolvers.jl:94-168) is a loop of outer Schur iterations,
+// each with an inner K-solve that is itself a loop (PCG, and for the
+// FP32-refined path a refinement loop around an FP32 PCG).  Every loop here
+// is a WHILE conditional graph node whose condition is set on the device by a
+// one-thread "check" kernel at the end of the body (cudaGraphSetConditional),
+// so a solve is one graph launch and one final synchronisation: no host
+// round-trip per iteration.  Stopping tests are the reference's:
+//   outer: ||r|| < rtol * ||r0|| and it >= itmin, or it == itmax,
+//          or breakdown (q.Sq <= 0 / non-finite) -> status
+//   inner: ||y - K z|| <= inner_rtol ||y|| or inner_itmax.
+// The captured sequence depends only on the hierarchy shape and the options
+// baked into it (precision, preconditioner, guess, rotation removal), so the
+// instantiated graph is cached in the context and reused across assemblies;
+// tolerances and iteration caps are read from device memory at run time.
+#include <cstring>
+#include <stdexcept>
+
+#include "kernels.cuh"
+#include "mg.cuh"
+#include "reduce.cuh"
+#include "solver.cuh"
+
+namespace dp {
+
+struct DevCtl {
+  // parameters (written by the host before each launch)
+  double rtol, inner_rtol, inner_rtol32, relax_cap;
+  int itmax, itmin, inner_itmax, max_refine;
+  // state
+  int outer_it, in_it, in32_it, ref_it, status, pad;
+  long long in_total, in32_total, ref_total;
+  double r0, tol, in_tol2, in32_tol2, ref_tol2;
+};
+
+enum GSlot { G_RZ = 16, G_RZN = 17, G_PAP = 18, G_IRR = 19, G_YY = 20,
+             F_RZ = 21, F_RZN = 22, F_PAP = 23, F_IRR = 24, F_YY = 25,
+             R_YY = 26, R_RES2 = 27, G_TMP3 = 28 };
+
+// ---- control kernels (one thread) ---------------------------------------------
+// Inner tolerance: fixed, or (relax) loosened in proportion to the outer
+// residual, rtol_k = min(cap, inner_rtol * ||r0|| / ||r_k||): an inexact-Krylov
+// relaxation that keeps the product of step size and inner error bounded.
+__device__ inline double inner_rtol_now(const DevCtl* ctl, const double* scal, int relax) {
+  double rt = ctl->inner_rtol;
+  if (relax && ctl->relax_cap > 0.0 && ctl->r0 > 0.0) {
+    const double rk = sqrt(scal[S_RR]);
+    if (rk > 0.0) rt = fmin(ctl->relax_cap, fmax(rt, rt * ctl->r0 / rk));
+  }
+  return rt;
+}
+
+__global__ void k_in_init(cudaGraphConditionalHandle h, DevCtl* ctl, const double* scal, int yy_slot, int irr_slot,
+                          double* scal_w, int fp32, int relax) {
+  const double yy = scal[yy_slot];
+  const double rt = fp32 ? ctl->inner_rtol32 : inner_rtol_now(ctl, scal, relax);
+  const double tol2 = rt * rt * yy;
+  if (fp32) { ctl->in32_it = 0; ctl->in32_tol2 = tol2; }
+  else { ctl->in_it = 0; ctl->in_tol2 = tol2; }
+  scal_w[irr_slot] = yy;
+  cudaGraphSetConditional(h, (yy > 0.0 && yy > tol2) ? 1u : 0u);
+}
+
+__global__ void k_in_check(cudaGraphConditionalHandle h, DevCtl* ctl, double* scal, int rz, int rzn, int irr, int fp32) {
+  int it;
+  double tol2;
+  if (fp32) { it = ++ctl->in32_it; tol2 = ctl->in32_tol2; ctl->in32_total += 1; }
+  else { it = ++ctl->in_it; tol2 = ctl->in_tol2; ctl->in_total += 1; }
+  scal[rz] = scal[rzn];
+  const double rr = scal[irr];
+  const bool go = isfinite(rr) && rr > tol2 && it < ctl->inner_itmax;
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+__global__ void k_ref_init(cudaGraphConditionalHandle h, DevCtl* ctl, double* scal, int relax) {
+  const double yy = scal[R_YY];
+  const double rt = inner_rtol_now(ctl, scal, relax);
+  ctl->ref_it = 0;
+  ctl->ref_tol2 = rt * rt * yy;
+  scal[R_RES2] = yy;
+  cudaGraphSetConditional(h, yy > 0.0 ? 1u : 0u);
+}
+
+__global__ void k_ref_check(cudaGraphConditionalHandle h, DevCtl* ctl, const double* scal) {
+  const int it = ++ctl->ref_it;
+  ctl->ref_total += 1;
+  const double rr = scal[R_RES2];
+  cudaGraphSetConditional(h, (isfinite(rr) && rr > ctl->ref_tol2 && it < ctl->max_refine) ? 1u : 0u);
+}
+
+__global__ void k_outer_init(cudaGraphConditionalHandle h, DevCtl* ctl, const double* scal) {
+  const double r0 = sqrt(scal[S_RR]);
+  ctl->r0 = r0;
+  ctl->tol = r0 * ctl->rtol;
+  ctl->outer_it = 0;
+  ctl->status = r0 > 0.0 ? 1 : 0;
+  cudaGraphSetConditional(h, (r0 > 0.0 && ctl->itmax >= 1) ? 1u : 0u);
+}
+
+__global__ void k_outer_check(cudaGraphConditionalHandle h, DevCtl* ctl, const double* scal) {
+  const int it = ++ctl->outer_it;
+  const double qsq = scal[S_QSQ], rd = scal[S_RD], rn = sqrt(scal[S_RR]);
+  unsigned go = 1u;
+  if (!(qsq > 0.0) || !isfinite(qsq) || !isfinite(rd) || !isfinite(rn)) {
+    ctl->status = 2;
+    go = 0u;
+  } else if (rn < ctl->tol && it >= ctl->itmin) {
+    ctl->status = 0;
+    go = 0u;
+  } else if (it >= ctl->itmax) {
+    go = 0u;
+  }
+  cudaGraphSetConditional(h, go);
+}
+
+// ---- PCG vector kernels reading their scalars from the table --------------------
+// p = z + beta p with beta = rzn/rz, except p = z on the first iteration
+template <typename T>
+__global__ void k_pcg_dir_g(T* __restrict__ p, const T* __restrict__ z, T* __restrict__ Ap, int64_t n,
+                            const double* scal, int rzn, int rz, const int* it) {
+  const double beta = (*it == 0) ? 0.0 : scal[rzn] / scal[rz];
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) {
+    p[i] = (T)((double)z[i] + beta * (double)p[i]);
+    Ap[i] = (T)0;  // the next apply accumulates into Ap
+  }
+}
+
+// FP64 residual -> FP32 hierarchy input, scaled by 1/||r|| (keeps FP32 in range)
+__global__ void k_r_to_f32(const double* __restrict__ r, float* __restrict__ r32, const double* scal, int irr, int64_t n) {
+  const double s = 1.0 / sqrt(scal[irr]);
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) r32[i] = (float)(s * r[i]);
+}
+__global__ void k_z_from_f32(const float* __restrict__ z32, double* __restrict__ z, const double* scal, int irr,
+                             int64_t n) {
+  const double s = sqrt(scal[irr]);
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) z[i] = s * (double)z32[i];
+}
+// nodal block Jacobi with an inverse of another precision
+template <typename Td, typename Tv>
+__global__ void k_bj_mixed(const Td* __restrict__ dinv, const Tv* __restrict__ r, Tv* __restrict__ z, int64_t nnod) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nnod) return;
+  double z0, z1;
+  bj_apply<Td>(dinv, n, (double)r[2 * n], (double)r[2 * n + 1], z0, z1);
+  z[2 * n] = (Tv)z0;
+  z[2 * n + 1] = (Tv)z1;
+}
+
+// x += alpha p; r -= alpha Ap; alpha = rzn/pAp; ||r||^2 -> irr
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_pcg_upd_g(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
+                                                            const T* __restrict__ Ap, int64_t n, double* scal, int rzn,
+                                                            int pap, int irr, double* partial, unsigned int* counter) {
+  const double alpha = scal[rzn] / scal[pap];
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
+    x[i] += (T)(alpha * (double)p[i]);
+    const double ri = (double)r[i] - alpha * (double)Ap[i];
+    r[i] = (T)ri;
+    s += ri * ri;
+  }
+  double v[1] = {s};
+  double* o[1] = {scal + irr};
+  grid_finish<1>(v, partial, counter, o);
+}
+
+__global__ void k_to_f32_scaled(const double* __restrict__ a, float* __restrict__ b, const double* scal, int64_t n) {
+  const double s = 1.0 / sqrt(scal[R_RES2]);
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)(s * a[i]);
+}
+__global__ void k_add_f32_scaled(double* __restrict__ z, const float* __restrict__ e, const double* scal, int64_t n) {
+  const double s = sqrt(scal[R_RES2]);
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) z[i] += s * (double)e[i];
+}
+
+// ---- capture helpers ---------------------------------------------------------------
+struct StreamSwap {
+  Ctx& c;
+  cudaStream_t saved;
+  StreamSwap(Ctx& cc, cudaStream_t s) : c(cc), saved(cc.stream) { c.stream = s; }
+  ~StreamSwap() { c.stream = saved; }
+};
+
+static cudaGraphConditionalHandle new_handle(cudaStream_t s) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  DP_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+  if (st != cudaStreamCaptureStatusActive) throw std::runtime_error("stream is not capturing");
+  cudaGraphConditionalHandle h;
+  DP_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+  return h;
+}
+
+// Appends a WHILE node on handle h at the current capture position of s and
+// returns its body graph.
+static cudaGraph_t add_while(cudaStream_t s, cudaGraphConditionalHandle h) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  DP_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  DP_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
+  DP_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+  return np.conditional.phGraph_out[0];
+}
+
+// Loop bodies by role, for the launch count: kernels per execution of each body.
+enum BodyRole { B_OUTER = 0, B_PCG64 = 1, B_PCG32 = 2, B_REF = 3 };
+
+// Captures emit() into body on the auxiliary stream of the given depth.
+template <typename F>
+static void capture_body(Ctx& c, cudaGraph_t body, int depth, int role, F&& emit) {
+  cudaStream_t aux = c.aux[depth];
+  DP_CUDA(cudaStreamBeginCaptureToGraph(aux, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  const int64_t start = g_klaunch;
+  const int64_t saved = c.cap_nested;
+  c.cap_nested = 0;
+  {
+    StreamSwap sw(c, aux);
+    emit();
+  }
+  cudaGraph_t out = nullptr;
+  DP_CUDA(cudaStreamEndCapture(aux, &out));
+  const int64_t all = g_klaunch - start;
+  c.gk_body[role] = all - c.cap_nested;   // kernels directly in this body
+  c.cap_nested = saved + all;             // the whole subtree is nested for the parent
+}
+
+static int g_nb(int64_t n) { return (int)div_up(n, 256); }
+
+// ---- emitted segments ----------------------------------------------------------------
+// PCG on K (precision T) for b -> x with preconditioner pc_kind; slots per precision.
+template <typename T>
+static void emit_pcg(Ctx& c, const SolveCfg& cfg, const T* Kmat, const T* b, T* x, T* r, T* z, T* p, T* Ap, int depth,
+                     int relax) {
+  const Level& L = c.fine;
+  const int64_t n = 2 * L.nnod;
+  const bool f32 = std::is_same<T, float>::value;
+  const int RZ = f32 ? F_RZ : G_RZ, RZN = f32 ? F_RZN : G_RZN, PAP = f32 ? F_PAP : G_PAP, IRR = f32 ? F_IRR : G_IRR,
+            YY = f32 ? F_YY : G_YY;
+  DevCtl* ctl = (DevCtl*)c.ctl;
+  DP_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * n, c.stream));
+  DP_CUDA(cudaMemcpyAsync(r, b, sizeof(T) * n, cudaMemcpyDeviceToDevice, c.stream));
+  if (f32) launch_dot_f(c, (const float*)b, (const float*)b, n, YY);
+  else launch_dot(c, (const double*)b, (const double*)b, n, YY);
+  cudaGraphConditionalHandle h = new_handle(c.stream);
+  ++g_klaunch;
+  k_in_init<<<1, 1, 0, c.stream>>>(h, ctl, c.scal, YY, IRR, c.scal, f32 ? 1 : 0, relax);
+  DP_LAUNCH_CHECK();
+  cudaGraph_t body = add_while(c.stream, h);
+  const int* itp = f32 ? &ctl->in32_it : &ctl->in_it;
+  capture_body(c, body, depth, f32 ? B_PCG32 : B_PCG64, [&] {
+    const bool mixed = !f32 && c.mg_prec == 1;  // FP64 Krylov, FP32 hierarchy
+    if (cfg.inner_pc == 0) {
+      if (f32) {
+        mg_apply_f(c, (const float*)r, (float*)z, cfg.mg);
+      } else if (mixed) {
+        float* r32 = (float*)c.work[W_F_R];
+        float* z32 = (float*)c.work[W_F_Z];
+        ++g_klaunch;
+        k_r_to_f32<<<g_nb(n), 256, 0, c.stream>>>((const double*)r, r32, c.scal, IRR, n);
+        mg_apply_f(c, r32, z32, cfg.mg);
+        ++g_klaunch;
+        k_z_from_f32<<<g_nb(n), 256, 0, c.stream>>>(z32, (double*)z, c.scal, IRR, n);
+      } else {
+        mg_apply(c, (const double*)r, (double*)z, cfg.mg);
+      }
+    } else {
+      ++g_klaunch;
+      if (c.mg_prec == 1) k_bj_mixed<float, T><<<g_nb(L.nnod), 256, 0, c.stream>>>(c.mg[0].dinv32, r, z, L.nnod);
+      else k_bj_mixed<double, T><<<g_nb(L.nnod), 256, 0, c.stream>>>(c.mg[0].dinv64, r, z, L.nnod);
+    }
+    if (f32) launch_dot_f(c, (const float*)r, (const float*)z, n, RZN);
+    else launch_dot(c, (const double*)r, (const double*)z, n, RZN);
+    ++g_klaunch;
+    k_pcg_dir_g<T><<<g_nb(n), 256, 0, c.stream>>>(p, z, Ap, n, c.scal, RZN, RZ, itp);
+    launch_apply_K_acc<T, T>(L, Kmat, p, Ap, c.stream);
+    if (f32) launch_dot_f(c, (const float*)p, (const float*)Ap, n, PAP);
+    else launch_dot(c, (const double*)p, (const double*)Ap, n, PAP);
+    ++g_klaunch;
+    k_pcg_upd_g<T><<<red_grid(n), kRedThreads, 0, c.stream>>>(x, r, p, Ap, n, c.scal, RZN, PAP, IRR, c.partial,
+                                                               c.counter);
+    ++g_klaunch;
+    k_in_check<<<1, 1, 0, c.stream>>>(h, ctl, c.scal, RZ, RZN, IRR, f32 ? 1 : 0);
+    DP_LAUNCH_CHECK();
+  });
+}
+
+// Inner solve K x = b (FP64 in/out) at capture depth `depth`.
+static void emit_inner(Ctx& c, const SolveCfg& cfg, const double* b, double* x, int depth, int relax) {
+  const int64_t n = 2 * c.fine.nnod;
+  if (cfg.precision <= 1) {
+    emit_pcg<double>(c, cfg, c.K64, b, x, (double*)c.work[W_IN_R], (double*)c.work[W_IN_Z], (double*)c.work[W_IN_P],
+                     (double*)c.work[W_IN_AP], depth, relax);
+    return;
+  }
+  DevCtl* ctl = (DevCtl*)c.ctl;
+  double* res = (double*)c.work[W_RES];
+  float* fb = (float*)c.work[W_F_B];
+  float* fx = (float*)c.work[W_F_X];
+  DP_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, c.stream));
+  DP_CUDA(cudaMemcpyAsync(res, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, c.stream));
+  launch_dot(c, b, b, n, R_YY);
+  cudaGraphConditionalHandle h = new_handle(c.stream);
+  ++g_klaunch;
+  k_ref_init<<<1, 1, 0, c.stream>>>(h, ctl, c.scal, relax);
+  DP_LAUNCH_CHECK();
+  cudaGraph_t body = add_while(c.stream, h);
+  capture_body(c, body, depth, B_REF, [&] {
+    ++g_klaunch;
+    k_to_f32_scaled<<<g_nb(n), 256, 0, c.stream>>>(res, fb, c.scal, n);
+    emit_pcg<float>(c, cfg, c.K32, fb, fx, (float*)c.work[W_F_R], (float*)c.work[W_F_Z], (float*)c.work[W_F_P],
+                    (float*)c.work[W_F_AP], depth + 1, 0);
+    ++g_klaunch;
+    k_add_f32_scaled<<<g_nb(n), 256, 0, c.stream>>>(x, fx, c.scal, n);
+    launch_apply_K<double, double>(c.fine, c.K64, x, res, c.stream);
+    ++g_klaunch;
+    k_residual<<<g_nb(n), 256, 0, c.stream>>>(b, res, n);
+    launch_dot(c, res, res, n, R_RES2);
+    ++g_klaunch;
+    k_ref_check<<<1, 1, 0, c.stream>>>(h, ctl, c.scal);
+    DP_LAUNCH_CHECK();
+  });
+}
+
+static void emit_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
+  const Level& L = c.fine;
+  const int64_t nU = 2 * L.nnod, nP = c.mesh.npres;
+  double* r = (double*)c.work[W_R];
+  double* rlast = (double*)c.work[W_RLAST];
+  double* d = (double*)c.work[W_D];
+  double* q = (double*)c.work[W_Q];
+  double* y = (double*)c.work[W_Y];
+  double* z = (double*)c.work[W_Z];
+  double* Sq = (double*)c.work[W_SQ];
+  double* rhs = (double*)c.work[W_RHS];
+  DevCtl* ctl = (DevCtl*)c.ctl;
+  DP_CUDA(cudaMemsetAsync(&ctl->in_total, 0, 3 * sizeof(long long), c.stream));
+  // Rhs = F + G P ; U = K^-1 Rhs
+  if (!cfg.use_guess) DP_CUDA(cudaMemsetAsync(P, 0, sizeof(double) * nP, c.stream));
+  launch_apply_G(c, P, y);
+  ++g_klaunch;
+  k_add<<<g_nb(nU), 256, 0, c.stream>>>(c.F, y, rhs, nU);
+  emit_inner(c, cfg, rhs, U, 0, 0);
+  // r = -G^T U ; rm0space!(r) ; ||r0||
+  launch_apply_GT(c, U, r);
+  ++g_klaunch;
+  k_neg<<<g_nb(nP), 256, 0, c.stream>>>(r, nP);
+  launch_sum(c, r, nP, S_SUMR);
+  ++g_klaunch;
+  k_sub_mean<<<g_nb(nP), 256, 0, c.stream>>>(r, nP, c.scal + S_SUMR);
+  launch_dot(c, r, r, nP, S_RR);
+  // d = r .* pc (or M^-1 r) ; q = d
+  if (cfg.schur_pc == 1) {
+    ++g_klaunch;
+    k_mass_blk<<<g_nb(L.nel), 256, 0, c.stream>>>(r, c.Minv, d, (int)L.nel);
+  } else {
+    ++g_klaunch;
+    k_mul_into<<<g_nb(nP), 256, 0, c.stream>>>(r, c.pc, d, nP);
+  }
+  DP_CUDA(cudaMemcpyAsync(q, d, sizeof(double) * nP, cudaMemcpyDeviceToDevice, c.stream));
+  launch_sum(c, q, nP, S_SUMQ);
+  cudaGraphConditionalHandle h = new_handle(c.stream);
+  ++g_klaunch;
+  k_outer_init<<<1, 1, 0, c.stream>>>(h, ctl, c.scal);
+  DP_LAUNCH_CHECK();
+  cudaGraph_t body = add_while(c.stream, h);
+  capture_body(c, body, 0, B_OUTER, [&] {
+    ++g_klaunch;
+    k_q_center_rd<<<red_grid(nP), kRedThreads, 0, c.stream>>>(q, r, d, nP, c.scal, c.partial, c.counter);
+    launch_apply_G(c, q, y);
+    emit_inner(c, cfg, y, z, 1, cfg.inner_relax > 0.0 ? 1 : 0);
+    launch_apply_GT(c, z, Sq);
+    launch_dot(c, q, Sq, nP, S_QSQ);
+    ++g_klaunch;
+    k_schur_update_p<<<red_grid(nP), kRedThreads, 0, c.stream>>>(P, r, rlast, q, Sq, nP, c.scal, c.partial, c.counter);
+    ++g_klaunch;
+    k_axpy_slot<<<g_nb(nU), 256, 0, c.stream>>>(U, z, nU, c.scal);
+    ++g_klaunch;
+    if (cfg.schur_pc == 1)
+      k_schur_center_blk<<<red_grid(L.nel), kRedThreads, 0, c.stream>>>(r, rlast, c.Minv, d, (int)L.nel, c.scal,
+                                                                         c.partial, c.counter);
+    else
+      k_schur_center<<<red_grid(nP), kRedThreads, 0, c.stream>>>(r, rlast, c.pc, d, nP, c.scal, c.partial, c.counter);
+    ++g_klaunch;
+    k_q_update<<<red_grid(nP), kRedThreads, 0, c.stream>>>(q, d, nP, c.scal, c.partial, c.counter);
+    ++g_klaunch;
+    k_outer_check<<<1, 1, 0, c.stream>>>(h, ctl, c.scal);
+    DP_LAUNCH_CHECK();
+  });
+  // diagnostics on the raw solution
+  launch_apply_K<double, double>(L, c.K64, U, rhs, c.stream);
+  launch_apply_G(c, P, y);
+  ++g_klaunch;
+  k_add<<<g_nb(nU), 256, 0, c.stream>>>(c.F, y, y, nU);
+  ++g_klaunch;
+  k_residual<<<g_nb(nU), 256, 0, c.stream>>>(y, rhs, nU);
+  launch_dot(c, rhs, rhs, nU, S_TMP);
+  launch_dot(c, c.F, c.F, nU, S_TMP2);
+  launch_apply_GT(c, U, Sq);
+  launch_sum(c, Sq, nP, S_SUMR);
+  ++g_klaunch;
+  k_sub_mean<<<g_nb(nP), 256, 0, c.stream>>>(Sq, nP, c.scal + S_SUMR);
+  launch_dot(c, Sq, Sq, nP, G_TMP3);
+  if (cfg.remove_rotation) {
+    ++g_klaunch;
+    k_rot_integrals<<<red_grid(L.nel), kRedThreads, 0, c.stream>>>(U, c.rho_lat, c.theta_lat, c.r_lat, (int)L.nel, L.ncr,
+                                                                   (int)L.A(), (int)L.B(), c.scal, c.partial, c.counter);
+    ++g_klaunch;
+    k_rot_remove<<<g_nb(L.nnod), 256, 0, c.stream>>>(U, c.r_lat, L.nnod, c.scal);
+  }
+  DP_LAUNCH_CHECK();
+}
+
+static int64_t graph_key(const SolveCfg& cfg, const Ctx& c) {
+  return (int64_t)cfg.precision | ((int64_t)cfg.inner_pc << 2) | ((int64_t)cfg.use_guess << 3) |
+         ((int64_t)cfg.remove_rotation << 4) | ((int64_t)c.mg_degree << 5) | ((int64_t)c.mg.size() << 9) |
+         ((int64_t)(cfg.inner_relax > 0.0) << 14) | ((int64_t)c.mg_prec << 15) | ((int64_t)cfg.schur_pc << 17);
+}
+
+void graph_free(Ctx& c) {
+  if (c.gexec) cudaGraphExecDestroy((cudaGraphExec_t)c.gexec);
+  if (c.graph) cudaGraphDestroy((cudaGraph_t)c.graph);
+  c.gexec = nullptr;
+  c.graph = nullptr;
+  c.gkey = -1;
+}
+
+int schur_pcg_graph(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& res) {
+  if (!c.ctl) {
+    DP_CUDA(cudaMalloc(&c.ctl, sizeof(DevCtl)));
+    DP_CUDA(cudaMallocHost(&c.h_ctl, sizeof(DevCtl)));
+    for (int i = 0; i < 3; ++i) DP_CUDA(cudaStreamCreateWithFlags(&c.aux[i], cudaStreamNonBlocking));
+  }
+  const int64_t key = graph_key(cfg, c);
+  if (!c.gexec || c.gkey != key || c.gU != U || c.gP != P) {
+    graph_free(c);
+    DP_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed));
+    const int64_t start = g_klaunch;
+    c.cap_nested = 0;
+    try {
+      emit_solve(c, cfg, U, P);
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(c.stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    cudaGraph_t g = nullptr;
+    DP_CUDA(cudaStreamEndCapture(c.stream, &g));
+    c.gk_main = (g_klaunch - start) - c.cap_nested;
+    cudaGraphExec_t ex = nullptr;
+    DP_CUDA(cudaGraphInstantiate(&ex, g, 0));
+    c.graph = g;
+    c.gexec = ex;
+    c.gkey = key;
+    c.gU = U;
+    c.gP = P;
+  }
+  DevCtl h{};
+  h.rtol = cfg.rtol;
+  h.inner_rtol = cfg.inner_rtol;
+  h.inner_rtol32 = cfg.inner_rtol32;
+  h.relax_cap = cfg.inner_relax;
+  h.itmax = cfg.itmax;
+  h.itmin = cfg.itmin;
+  h.inner_itmax = cfg.inner_itmax;
+  h.max_refine = cfg.max_refine;
+  *(DevCtl*)c.h_ctl = h;
+  DP_CUDA(cudaMemcpyAsync(c.ctl, c.h_ctl, sizeof(DevCtl), cudaMemcpyHostToDevice, c.stream));
+  DP_CUDA(cudaGraphLaunch((cudaGraphExec_t)c.gexec, c.stream));
+  DP_CUDA(cudaMemcpyAsync(c.h_ctl, c.ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, c.stream));
+  DP_CUDA(cudaMemcpyAsync(c.h_scal, c.scal, sizeof(double) * 32, cudaMemcpyDeviceToHost, c.stream));
+  DP_CUDA(cudaStreamSynchronize(c.stream));
+  const DevCtl& o = *(const DevCtl*)c.h_ctl;
+  res.status = o.status;
+  res.iterations = o.outer_it;
+  res.inner_its = cfg.precision == 2 ? o.in32_total : o.in_total;
+  res.launches = c.gk_main + c.gk_body[B_OUTER] * o.outer_it + c.gk_body[B_PCG64] * o.in_total +
+                 c.gk_body[B_PCG32] * o.in32_total + c.gk_body[B_REF] * o.ref_total;
+  res.refinements = o.ref_total;
+  res.r0 = o.r0;
+  res.relres = o.r0 > 0 ? std::sqrt(c.h_scal[S_RR]) / o.r0 : 0.0;
+  res.mom_residual = std::sqrt(c.h_scal[S_TMP] / std::max(c.h_scal[S_TMP2], 1e-300));
+  res.div_residual = o.r0 > 0 ? std::sqrt(c.h_scal[G_TMP3]) / o.r0 : 0.0;
+  res.omega = cfg.remove_rotation ? c.h_scal[S_AM] / c.h_scal[S_MOM] : 0.0;
+  return res.status;
+}
+
+}  // namespace dp

@@ -19,6 +19,7 @@
 // inverted once per setup and applied as a dense mat-vec.
 #include <algorithm>
 #include <cmath>
+#include <stdexcept>
 
 #include "kernels.cuh"
 #include "mg.cuh"
@@ -59,6 +60,68 @@ static void coarse_ref(int type, double alpha, double beta, double* xi, double* 
   }
 }
 
+// Restriction stencils.  R = P^T is translation invariant on the structured
+// lattice: the fine nodes inside the support of a coarse basis function, and
+// their weights, depend only on the parity class (a_c mod 2, b_c mod 2) of the
+// coarse node.  The table is built once from the prolongation rule on an
+// interior node of each class; at the walls the fine nodes outside the annulus
+// are simply absent.  This turns the restriction into a gather (no atomics,
+// no zeroing pass, deterministic).
+constexpr int kRMax = 64;
+struct RestrictTable {
+  int n[4];
+  signed char da[4][kRMax], db[4][kRMax];
+  double w[4][kRMax];
+};
+__constant__ RestrictTable c_rtab;
+
+static void host_fine_weights(int a, int b, int ncrc, int Ac, int Bc, int cn[6], double w[6]) {
+  int IR = a >> 2;
+  if (IR >= ncrc) IR = ncrc - 1;
+  const int IT = b >> 2;
+  const int alpha = a - 4 * IR, beta = b - 4 * IT;
+  const int ct = (alpha + beta <= 4) ? 0 : 1;
+  double xi, eta;
+  coarse_ref(ct, alpha, beta, &xi, &eta);
+  p2_values(xi, eta, w);
+  for (int k = 0; k < 6; ++k) {
+    const int ac = 2 * IR + kLocA[ct][k];
+    int bc = 2 * IT + kLocB[ct][k];
+    if (bc >= Bc) bc -= Bc;
+    cn[k] = ac + Ac * bc;
+  }
+}
+
+static void upload_restriction_table() {
+  RestrictTable R{};
+  const int ncrc = 8, nctc = 16, Ac = 2 * ncrc + 1, Bc = 2 * nctc, Af = 4 * ncrc + 1, Bf = 4 * nctc;
+  for (int cls = 0; cls < 4; ++cls) {
+    const int ac = 8 + (cls & 1), bc = 12 + (cls >> 1);
+    const int target = ac + Ac * bc;
+    int m = 0;
+    for (int da = -4; da <= 4; ++da)
+      for (int db = -4; db <= 4; ++db) {
+        const int a = 2 * ac + da, b = 2 * bc + db;
+        if (a < 0 || a >= Af || b < 0 || b >= Bf) continue;
+        int cn[6];
+        double w[6];
+        host_fine_weights(a, b, ncrc, Ac, Bc, cn, w);
+        double wt = 0.0;
+        for (int k = 0; k < 6; ++k)
+          if (cn[k] == target) wt += w[k];
+        if (wt != 0.0) {
+          if (m >= kRMax) throw std::runtime_error("restriction table overflow");
+          R.da[cls][m] = (signed char)da;
+          R.db[cls][m] = (signed char)db;
+          R.w[cls][m] = wt;
+          ++m;
+        }
+      }
+    R.n[cls] = m;
+  }
+  DP_CUDA(cudaMemcpyToSymbol(c_rtab, &R, sizeof(R)));
+}
+
 void upload_mg_constants() {
   ChildTable T{};
   // coarse A children: (0,0,A) (0,0,B) (0,1,A) (1,0,A); coarse B: (0,1,B) (1,0,B) (1,1,A) (1,1,B)
@@ -80,6 +143,7 @@ void upload_mg_constants() {
       }
     }
   DP_CUDA(cudaMemcpyToSymbol(c_child, &T, sizeof(T)));
+  upload_restriction_table();
 }
 
 // ---- Galerkin coarsening: one thread per (coarse element, packed entry) ------
@@ -129,23 +193,57 @@ __global__ void k_galerkin(const T* __restrict__ Kf, T* __restrict__ Kc, int nel
   Kc[(size_t)pidx * nelc + E] = (T)acc;
 }
 
-// ---- diagonal --------------------------------------------------------------
+// ---- nodal 2x2 diagonal blocks and their inverses ----------------------------
 template <typename T>
-__global__ void k_diag(const T* __restrict__ K, double* __restrict__ diag, int nel, int ncr, int A, int B) {
+__global__ void k_diag_blocks(const T* __restrict__ K, double* __restrict__ diag, int nel, int ncr, int A, int B) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nel) return;
   int nd[6];
   element_nodes_mg(e, ncr, A, B, nd);
 #pragma unroll
-  for (int d = 0; d < 12; ++d) atomicAdd(&diag[2 * nd[d >> 1] + (d & 1)], (double)K[(size_t)packed_index12(d, d) * nel + e]);
+  for (int k = 0; k < 6; ++k) {
+    atomicAdd(&diag[3 * nd[k] + 0], (double)K[(size_t)packed_index12(2 * k, 2 * k) * nel + e]);
+    atomicAdd(&diag[3 * nd[k] + 1], (double)K[(size_t)packed_index12(2 * k + 1, 2 * k) * nel + e]);
+    atomicAdd(&diag[3 * nd[k] + 2], (double)K[(size_t)packed_index12(2 * k + 1, 2 * k + 1) * nel + e]);
+  }
+}
+
+// Inverse of the nodal block (block = 1) or of its diagonal (block = 0);
+// constrained DOFs get zero rows/columns so the smoother never touches them.
+template <typename T>
+__global__ void k_block_invert(const double* __restrict__ diag, T* __restrict__ dinv, int64_t nnod, int A, int pin,
+                               int block) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nnod) return;
+  const int a = (int)(n % A), b = (int)(n / A);
+  const bool f0 = dof_fixed(a, b, 0, A - 1, pin), f1 = dof_fixed(a, b, 1, A - 1, pin);
+  const double d00 = diag[3 * n], d11 = diag[3 * n + 2];
+  double d01 = block ? diag[3 * n + 1] : 0.0;
+  double i00 = 0.0, i01 = 0.0, i11 = 0.0;
+  if (f0 || f1 || d01 == 0.0) {
+    i00 = (!f0 && d00 > 0.0) ? 1.0 / d00 : 0.0;
+    i11 = (!f1 && d11 > 0.0) ? 1.0 / d11 : 0.0;
+  } else {
+    const double det = d00 * d11 - d01 * d01;
+    if (det > 0.0) {
+      i00 = d11 / det;
+      i01 = -d01 / det;
+      i11 = d00 / det;
+    } else {
+      i00 = d00 > 0.0 ? 1.0 / d00 : 0.0;
+      i11 = d11 > 0.0 ? 1.0 / d11 : 0.0;
+    }
+  }
+  dinv[3 * n] = (T)i00;
+  dinv[3 * n + 1] = (T)i01;
+  dinv[3 * n + 2] = (T)i11;
 }
 
 template <typename T>
-__global__ void k_diag_invert(const double* __restrict__ diag, T* __restrict__ dinv, int64_t n) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double d = diag[i];
-  dinv[i] = (T)(d > 0.0 ? 1.0 / d : 0.0);
+__device__ inline void bj_apply(const T* __restrict__ dinv, int64_t n, double r0, double r1, double& z0, double& z1) {
+  const double a = (double)dinv[3 * n], b = (double)dinv[3 * n + 1], c = (double)dinv[3 * n + 2];
+  z0 = a * r0 + b * r1;
+  z1 = b * r0 + c * r1;
 }
 
 // ---- transfers ---------------------------------------------------------------
@@ -175,10 +273,11 @@ __device__ inline void fine_node_weights(int a, int b, int ncrc, int Ac, int Bc,
   }
 }
 
-// xf += P xc (per fine node, gather)
+// xf += P xc (per fine node, gather); also zeroes zb (the fine level's residual
+// buffer, which the next apply accumulates into)
 template <typename T>
-__global__ void k_prolong_add(const T* __restrict__ xc, T* __restrict__ xf, int Af, int Bf, int ncrc, int Ac, int Bc,
-                              int pin) {
+__global__ void k_prolong_add(const T* __restrict__ xc, T* __restrict__ xf, T* __restrict__ zb, int Af, int Bf,
+                              int ncrc, int Ac, int Bc, int pin) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= Af * Bf) return;
   const int a = n % Af, b = n / Af;
@@ -195,84 +294,100 @@ __global__ void k_prolong_add(const T* __restrict__ xc, T* __restrict__ xf, int 
   }
   if (!dof_fixed(a, b, 0, Af - 1, pin)) xf[2 * n] += (T)s0;
   if (!dof_fixed(a, b, 1, Af - 1, pin)) xf[2 * n + 1] += (T)s1;
+  zb[2 * n] = (T)0;
+  zb[2 * n + 1] = (T)0;
 }
 
-// bc = P^T rf (per fine node scatter), bc zeroed by the caller
+// bc = P^T (r - t) per coarse node (gather over the class stencil); constrained
+// DOFs of either level are excluded.
 template <typename T>
-__global__ void k_restrict(const T* __restrict__ rf, T* __restrict__ bc, int Af, int Bf, int ncrc, int Ac, int Bc,
-                           int pin) {
+__global__ void k_restrict_g(const T* __restrict__ r, const T* __restrict__ t, T* __restrict__ bc, int Af, int Bf,
+                             int Ac, int Bc, int pin) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= Af * Bf) return;
-  const int a = n % Af, b = n / Af;
-  int cn[6];
-  double w[6];
-  fine_node_weights(a, b, ncrc, Ac, Bc, cn, w);
-  const double r0 = dof_fixed(a, b, 0, Af - 1, pin) ? 0.0 : (double)rf[2 * n];
-  const double r1 = dof_fixed(a, b, 1, Af - 1, pin) ? 0.0 : (double)rf[2 * n + 1];
-#pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    if (w[k] != 0.0) {
-      atomicAdd(&bc[2 * cn[k]], (T)(w[k] * r0));
-      atomicAdd(&bc[2 * cn[k] + 1], (T)(w[k] * r1));
-    }
+  if (n >= Ac * Bc) return;
+  const int ac = n % Ac, bcn = n / Ac;
+  const int cls = (ac & 1) | ((bcn & 1) << 1);
+  const int m = c_rtab.n[cls];
+  double s0 = 0.0, s1 = 0.0;
+  for (int j = 0; j < m; ++j) {
+    const int a = 2 * ac + c_rtab.da[cls][j];
+    if (a < 0 || a >= Af) continue;
+    int b = 2 * bcn + c_rtab.db[cls][j];
+    if (b < 0) b += Bf;
+    if (b >= Bf) b -= Bf;
+    const int f = a + Af * b;
+    const double w = c_rtab.w[cls][j];
+    if (!dof_fixed(a, b, 0, Af - 1, pin)) s0 += w * ((double)r[2 * f] - (double)t[2 * f]);
+    if (!dof_fixed(a, b, 1, Af - 1, pin)) s1 += w * ((double)r[2 * f + 1] - (double)t[2 * f + 1]);
   }
+  bc[2 * n] = dof_fixed(ac, bcn, 0, Ac - 1, pin) ? (T)0 : (T)s0;
+  bc[2 * n + 1] = dof_fixed(ac, bcn, 1, Ac - 1, pin) ? (T)0 : (T)s1;
 }
 
-// zero the constrained DOFs: wall u_r (2*B of them) and the pinned u_theta
-template <typename T>
-__global__ void k_mask_fixed(T* __restrict__ v, int A, int B, int pin) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n == 2 * B) {
-    if (pin) v[2 * (A - 1)] = (T)0;
-    return;
-  }
-  if (n > 2 * B) return;
-  const int b = n >> 1;
-  const int a = (n & 1) ? A - 1 : 0;
-  v[2 * (a + A * b) + 1] = (T)0;
-}
-
-// ---- Chebyshev smoother vector steps -----------------------------------------
+// ---- Chebyshev smoother vector steps (per node, coefficients read from device) --
 // first step from x = 0: r = b, d = (1/theta) D^-1 b, x = d
+// (every Chebyshev kernel also zeroes t, which the next apply accumulates into)
 template <typename T>
 __global__ void k_cheb_first(const T* __restrict__ b, const T* __restrict__ dinv, T* __restrict__ x,
-                             T* __restrict__ r, T* __restrict__ d, double inv_theta, int64_t n) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const T bi = b[i];
-  const T di = (T)(inv_theta * (double)dinv[i] * (double)bi);
-  r[i] = bi;
-  d[i] = di;
-  x[i] = di;
+                             T* __restrict__ r, T* __restrict__ d, T* __restrict__ t, const double* __restrict__ coef,
+                             int64_t nnod) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nnod) return;
+  t[2 * n] = (T)0; t[2 * n + 1] = (T)0;
+  const double it = coef[0];
+  const double b0 = (double)b[2 * n], b1 = (double)b[2 * n + 1];
+  double z0, z1;
+  bj_apply<T>(dinv, n, b0, b1, z0, z1);
+  r[2 * n] = (T)b0; r[2 * n + 1] = (T)b1;
+  d[2 * n] = (T)(it * z0); d[2 * n + 1] = (T)(it * z1);
+  x[2 * n] = (T)(it * z0); x[2 * n + 1] = (T)(it * z1);
 }
 // first step from a given x: r = b - Ax (Ax in r on entry), d = (1/theta) D^-1 r, x += d
 template <typename T>
 __global__ void k_cheb_first_x(const T* __restrict__ b, const T* __restrict__ dinv, T* __restrict__ x,
-                               T* __restrict__ r, T* __restrict__ d, double inv_theta, int64_t n) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const T ri = b[i] - r[i];
-  const T di = (T)(inv_theta * (double)dinv[i] * (double)ri);
-  r[i] = ri;
-  d[i] = di;
-  x[i] += di;
+                               T* __restrict__ r, T* __restrict__ d, T* __restrict__ t,
+                               const double* __restrict__ coef, int64_t nnod) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nnod) return;
+  t[2 * n] = (T)0; t[2 * n + 1] = (T)0;
+  const double it = coef[0];
+  const double r0 = (double)b[2 * n] - (double)r[2 * n], r1 = (double)b[2 * n + 1] - (double)r[2 * n + 1];
+  double z0, z1;
+  bj_apply<T>(dinv, n, r0, r1, z0, z1);
+  r[2 * n] = (T)r0; r[2 * n + 1] = (T)r1;
+  d[2 * n] = (T)(it * z0); d[2 * n + 1] = (T)(it * z1);
+  x[2 * n] += (T)(it * z0); x[2 * n + 1] += (T)(it * z1);
 }
-// r -= Ad; d = c1 d + c2 D^-1 r; x += d
+// r -= Ad; d = c1 d + c2 D^-1 r; x += d  (c1, c2 = coef[0], coef[1])
 template <typename T>
-__global__ void k_cheb_step(const T* __restrict__ Ad, const T* __restrict__ dinv, T* __restrict__ x,
-                            T* __restrict__ r, T* __restrict__ d, double c1, double c2, int64_t n) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const T ri = r[i] - Ad[i];
-  const T di = (T)(c1 * (double)d[i] + c2 * (double)dinv[i] * (double)ri);
-  r[i] = ri;
-  d[i] = di;
-  x[i] += di;
+__global__ void k_cheb_step(T* __restrict__ Ad, const T* __restrict__ dinv, T* __restrict__ x,
+                            T* __restrict__ r, T* __restrict__ d, const double* __restrict__ coef, int64_t nnod) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nnod) return;
+  const double c1 = coef[0], c2 = coef[1];
+  const double r0 = (double)r[2 * n] - (double)Ad[2 * n], r1 = (double)r[2 * n + 1] - (double)Ad[2 * n + 1];
+  Ad[2 * n] = (T)0; Ad[2 * n + 1] = (T)0;
+  double z0, z1;
+  bj_apply<T>(dinv, n, r0, r1, z0, z1);
+  const double d0 = c1 * (double)d[2 * n] + c2 * z0, d1 = c1 * (double)d[2 * n + 1] + c2 * z1;
+  r[2 * n] = (T)r0; r[2 * n + 1] = (T)r1;
+  d[2 * n] = (T)d0; d[2 * n + 1] = (T)d1;
+  x[2 * n] += (T)d0; x[2 * n + 1] += (T)d1;
 }
 template <typename T>
 __global__ void k_sub(const T* __restrict__ b, T* __restrict__ r, int64_t n) {  // r = b - r
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) r[i] = b[i] - r[i];
+}
+// z = D^-1 r (nodal blocks)
+template <typename T>
+__global__ void k_bj(const T* __restrict__ dinv, const T* __restrict__ r, T* __restrict__ z, int64_t nnod) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nnod) return;
+  double z0, z1;
+  bj_apply<T>(dinv, n, (double)r[2 * n], (double)r[2 * n + 1], z0, z1);
+  z[2 * n] = (T)z0;
+  z[2 * n + 1] = (T)z1;
 }
 
 // ---- coarse dense solve --------------------------------------------------------
@@ -361,7 +476,7 @@ void mg_free(Ctx& c) {
   for (size_t l = 0; l < c.mg.size(); ++l) {
     MGLevel& L = c.mg[l];
     if (l > 0) { cudaFree(L.K64); cudaFree(L.K32); }
-    cudaFree(L.dinv64); cudaFree(L.dinv32);
+    cudaFree(L.dinv64); cudaFree(L.dinv32); cudaFree(L.cheb);
     cudaFree(L.x); cudaFree(L.b); cudaFree(L.r); cudaFree(L.d); cudaFree(L.t);
   }
   c.mg.clear();
@@ -426,24 +541,26 @@ __global__ void k_fill_pattern(T* v, int64_t n, int A, int pin) {
 }
 
 template <typename T>
-__global__ void k_pcg_vec(T* __restrict__ x, T* __restrict__ r, T* __restrict__ p, const T* __restrict__ Ap,
-                          const T* __restrict__ dinv, T* __restrict__ z, double alpha, int64_t n) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  x[i] += (T)(alpha * (double)p[i]);
-  const T ri = r[i] - (T)(alpha * (double)Ap[i]);
-  r[i] = ri;
-  z[i] = dinv[i] * ri;
+__global__ void k_pcg_vec(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p, const T* __restrict__ Ap,
+                          const T* __restrict__ dinv, T* __restrict__ z, double alpha, int64_t nnod) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nnod) return;
+  double rr[2];
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    x[2 * n + c] += (T)(alpha * (double)p[2 * n + c]);
+    rr[c] = (double)r[2 * n + c] - alpha * (double)Ap[2 * n + c];
+    r[2 * n + c] = (T)rr[c];
+  }
+  double z0, z1;
+  bj_apply<T>(dinv, n, rr[0], rr[1], z0, z1);
+  z[2 * n] = (T)z0;
+  z[2 * n + 1] = (T)z1;
 }
 template <typename T>
 __global__ void k_xpby(const T* __restrict__ z, T* __restrict__ p, double beta, int64_t n) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) p[i] = z[i] + (T)(beta * (double)p[i]);
-}
-template <typename T>
-__global__ void k_mul(const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ out, int64_t n) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < n) out[i] = a[i] * b[i];
 }
 
 // lambda_max(D^-1 A) from 10 steps of Jacobi-PCG (Lanczos coefficients).
@@ -453,8 +570,10 @@ static double estimate_lmax(Ctx& c, MGLevel& L) {
   T* x = (T*)L.x; T* r = (T*)L.r; T* p = (T*)L.d; T* z = (T*)L.b; T* Ap = (T*)L.t;
   const T* dinv = level_dinv<T>(L);
   DP_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * n, c.stream));
+  ++g_klaunch;
   k_fill_pattern<T><<<tpb(n), 256, 0, c.stream>>>(r, n, (int)L.g.A(), L.g.pin);
-  k_mul<T><<<tpb(n), 256, 0, c.stream>>>(dinv, r, z, n);
+  ++g_klaunch;
+  k_bj<T><<<tpb(L.g.nnod), 256, 0, c.stream>>>(dinv, r, z, L.g.nnod);
   DP_CUDA(cudaMemcpyAsync(p, z, sizeof(T) * n, cudaMemcpyDeviceToDevice, c.stream));
   dot_level<T>(c, r, z, n, 20);
   DP_CUDA(cudaMemcpyAsync(c.h_scal + 20, c.scal + 20, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
@@ -470,7 +589,8 @@ static double estimate_lmax(Ctx& c, MGLevel& L) {
     const double pAp = c.h_scal[21];
     if (!(pAp > 0.0)) break;
     const double alpha = rz / pAp;
-    k_pcg_vec<T><<<tpb(n), 256, 0, c.stream>>>(x, r, p, Ap, dinv, z, alpha, n);
+    ++g_klaunch;
+    k_pcg_vec<T><<<tpb(L.g.nnod), 256, 0, c.stream>>>(x, r, p, Ap, dinv, z, alpha, L.g.nnod);
     dot_level<T>(c, r, z, n, 20);
     DP_CUDA(cudaMemcpyAsync(c.h_scal + 20, c.scal + 20, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     DP_CUDA(cudaStreamSynchronize(c.stream));
@@ -480,6 +600,7 @@ static double estimate_lmax(Ctx& c, MGLevel& L) {
     betas.push_back(beta);
     rz = rz_new;
     if (!(rz > 0.0)) break;
+    ++g_klaunch;
     k_xpby<T><<<tpb(n), 256, 0, c.stream>>>(z, p, beta, n);
   }
   DP_LAUNCH_CHECK();
@@ -507,7 +628,7 @@ template <typename T>
 static void mg_setup_t(Ctx& c, const MGOptions& o) {
   const int prec = std::is_same<T, float>::value ? 1 : 0;
   // level geometry (reuse if unchanged)
-  if (c.mg.empty() || c.mg_prec != prec) {
+  if (c.mg.empty() || c.mg_prec != prec || c.mg_coarse_max != o.coarse_max) {
     mg_free(c);
     MGLevel L0;
     L0.g = c.fine;
@@ -532,7 +653,8 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
       if (l > 0) {
         DP_CUDA(cudaMalloc(prec ? (void**)&L.K32 : (void**)&L.K64, sizeof(T) * kKe * L.g.nel));
       }
-      DP_CUDA(cudaMalloc(prec ? (void**)&L.dinv32 : (void**)&L.dinv64, sizeof(T) * 2 * L.g.nnod));
+      DP_CUDA(cudaMalloc(prec ? (void**)&L.dinv32 : (void**)&L.dinv64, sizeof(T) * 3 * L.g.nnod));
+      DP_CUDA(cudaMalloc(&L.cheb, sizeof(double) * 2 * (kMaxCheb + 1)));
       setup_level_vectors<T>(L);
     }
     c.coarse_n = 2 * c.mg.back().g.nnod;
@@ -542,6 +664,7 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
       c.coarse_n = 0;
     }
     c.mg_prec = prec;
+    c.mg_coarse_max = o.coarse_max;
   }
   // fine operator pointer
   if (prec) c.mg[0].K32 = c.K32; else c.mg[0].K64 = c.K64;
@@ -550,25 +673,46 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
     MGLevel& Lf = c.mg[l - 1];
     MGLevel& Lc = c.mg[l];
     const int64_t nthreads = Lc.g.nel * kKe;
+    ++g_klaunch;
     k_galerkin<T><<<(int)div_up(nthreads, 128), 128, 0, c.stream>>>(level_K<T>(Lf), level_K<T>(Lc), (int)Lc.g.nel,
                                                                       Lc.g.ncr, Lc.g.nct, (int)Lf.g.nel, Lf.g.ncr,
                                                                       Lc.g.pin);
     DP_LAUNCH_CHECK();
   }
-  // diagonals + eigenvalue estimates
+  // nodal diagonal blocks, eigenvalue estimates and Chebyshev coefficients
   double* diag = nullptr;
-  DP_CUDA(cudaMalloc(&diag, sizeof(double) * 2 * c.mg[0].g.nnod));
+  DP_CUDA(cudaMalloc(&diag, sizeof(double) * 3 * c.mg[0].g.nnod));
+  const int deg = std::max(1, std::min(o.cheb_degree, kMaxCheb));
   for (size_t l = 0; l < c.mg.size(); ++l) {
     MGLevel& L = c.mg[l];
-    const int64_t n = 2 * L.g.nnod;
-    DP_CUDA(cudaMemsetAsync(diag, 0, sizeof(double) * n, c.stream));
-    k_diag<T><<<(int)div_up(L.g.nel, 128), 128, 0, c.stream>>>(level_K<T>(L), diag, (int)L.g.nel, L.g.ncr,
-                                                                (int)L.g.A(), (int)L.g.B());
-    k_diag_invert<T><<<tpb(n), 256, 0, c.stream>>>(diag, level_dinv<T>(L), n);
+    DP_CUDA(cudaMemsetAsync(diag, 0, sizeof(double) * 3 * L.g.nnod, c.stream));
+    ++g_klaunch;
+    k_diag_blocks<T><<<(int)div_up(L.g.nel, 128), 128, 0, c.stream>>>(level_K<T>(L), diag, (int)L.g.nel, L.g.ncr,
+                                                                       (int)L.g.A(), (int)L.g.B());
+    ++g_klaunch;
+    k_block_invert<T><<<tpb(L.g.nnod), 256, 0, c.stream>>>(diag, level_dinv<T>(L), L.g.nnod, (int)L.g.A(), L.g.pin,
+                                                            o.block_jacobi);
     DP_LAUNCH_CHECK();
     const bool is_coarsest_direct = (l + 1 == c.mg.size()) && c.coarse_n > 0;
     L.lmax = is_coarsest_direct ? 0.0 : estimate_lmax<T>(c, L);
+    // Chebyshev recurrence coefficients on [lo, hi] * lmax (three-term form)
+    double coef[2 * (kMaxCheb + 1)] = {0.0};
+    if (L.lmax > 0.0) {
+      const double lmx = o.cheb_hi * L.lmax, lmn = o.cheb_lo * L.lmax;
+      const double theta = 0.5 * (lmx + lmn), delta = 0.5 * (lmx - lmn), sigma = theta / delta;
+      double rho_prev = 1.0 / sigma;
+      coef[0] = 1.0 / theta;
+      for (int k = 1; k < deg; ++k) {
+        const double rho = 1.0 / (2.0 * sigma - rho_prev);
+        coef[2 * k] = rho * rho_prev;
+        coef[2 * k + 1] = 2.0 * rho / delta;
+        rho_prev = rho;
+      }
+    }
+    DP_CUDA(cudaMemcpyAsync(L.cheb, coef, sizeof(coef), cudaMemcpyHostToDevice, c.stream));
+    DP_CUDA(cudaStreamSynchronize(c.stream));
   }
+  c.mg_degree = deg;
   DP_CUDA(cudaFree(diag));
   // coarse dense inverse
   if (c.coarse_n > 0) {
@@ -578,9 +722,12 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
     double* Inv = D + (size_t)n * n;
     double* tmp = Inv + (size_t)n * n;
     DP_CUDA(cudaMemsetAsync(D, 0, sizeof(double) * n * n, c.stream));
+    ++g_klaunch;
     k_dense_assemble<T><<<(int)div_up(L.g.nel, 128), 128, 0, c.stream>>>(level_K<T>(L), D, (int)L.g.nel, L.g.ncr,
                                                                           (int)L.g.A(), (int)L.g.B(), n);
+    ++g_klaunch;
     k_dense_cholesky<<<1, 1024, 0, c.stream>>>(D, n);
+    ++g_klaunch;
     k_dense_inverse<<<(int)div_up(n, 64), 64, 0, c.stream>>>(D, Inv, tmp, n);
     DP_LAUNCH_CHECK();
   }
@@ -591,27 +738,28 @@ void mg_setup(Ctx& c, int precision, const MGOptions& o) {
   else mg_setup_t<double>(c, o);
 }
 
-// Chebyshev smoothing of A x = b on level L; x_zero: start from x = 0.
+// Chebyshev smoothing of A x = b on level L.  x_zero: start from x = 0.
+// Otherwise L.r must hold zeros on entry (the prolongation zeroes it).  The
+// recurrence coefficients live in L.cheb on the device, so this sequence is
+// the same for every assembly and is captured once into the solve graph.
+// On exit r = b - A (x - d_last), i.e. the true residual is r - A d_last.
 template <typename T>
-static void chebyshev(Ctx& c, MGLevel& L, const T* b, T* x, bool x_zero, const MGOptions& o) {
-  const int64_t n = 2 * L.g.nnod;
-  const double lmax = o.cheb_hi * L.lmax, lmin = o.cheb_lo * L.lmax;
-  const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
-  const double sigma = theta / delta;
-  double rho_prev = 1.0 / sigma;
+static void chebyshev(Ctx& c, MGLevel& L, const T* b, T* x, bool x_zero) {
+  const int64_t nn = L.g.nnod;
   T* r = (T*)L.r; T* d = (T*)L.d; T* Ad = (T*)L.t;
   const T* dinv = level_dinv<T>(L);
   if (x_zero) {
-    k_cheb_first<T><<<tpb(n), 256, 0, c.stream>>>(b, dinv, x, r, d, 1.0 / theta, n);
+    ++g_klaunch;
+    k_cheb_first<T><<<tpb(nn), 256, 0, c.stream>>>(b, dinv, x, r, d, Ad, L.cheb, nn);
   } else {
-    apply_level<T>(c, L, x, r);
-    k_cheb_first_x<T><<<tpb(n), 256, 0, c.stream>>>(b, dinv, x, r, d, 1.0 / theta, n);
+    launch_apply_K_acc<T, T>(L.g, level_K<T>(L), x, r, c.stream);
+    ++g_klaunch;
+    k_cheb_first_x<T><<<tpb(nn), 256, 0, c.stream>>>(b, dinv, x, r, d, Ad, L.cheb, nn);
   }
-  for (int k = 1; k < o.cheb_degree; ++k) {
-    apply_level<T>(c, L, d, Ad);
-    const double rho = 1.0 / (2.0 * sigma - rho_prev);
-    k_cheb_step<T><<<tpb(n), 256, 0, c.stream>>>(Ad, dinv, x, r, d, rho * rho_prev, 2.0 * rho / delta, n);
-    rho_prev = rho;
+  for (int k = 1; k < c.mg_degree; ++k) {
+    launch_apply_K_acc<T, T>(L.g, level_K<T>(L), d, Ad, c.stream);
+    ++g_klaunch;
+    k_cheb_step<T><<<tpb(nn), 256, 0, c.stream>>>(Ad, dinv, x, r, d, L.cheb + 2 * k, nn);
   }
   DP_LAUNCH_CHECK();
 }
@@ -619,39 +767,41 @@ static void chebyshev(Ctx& c, MGLevel& L, const T* b, T* x, bool x_zero, const M
 template <typename T>
 static void vcycle(Ctx& c, size_t l, const T* b, T* x, const MGOptions& o) {
   MGLevel& L = c.mg[l];
-  const int64_t n = 2 * L.g.nnod;
   if (l + 1 == c.mg.size()) {
     if (c.coarse_n > 0) {
+      // dense inverse: identity rows on constrained DOFs keep them at zero
       const int nn = (int)c.coarse_n;
       const double* Inv = c.coarse_chol + (size_t)nn * nn;
+      ++g_klaunch;
       k_dense_apply<T><<<(int)div_up(nn, 8), 256, 0, c.stream>>>(Inv, b, x, nn);
-      k_mask_fixed<T><<<tpb(2 * L.g.B() + 1), 256, 0, c.stream>>>(x, (int)L.g.A(), (int)L.g.B(), L.g.pin);
       DP_LAUNCH_CHECK();
     } else {
-      chebyshev<T>(c, L, b, x, true, o);
-      for (int s = 1; s < o.coarse_sweeps; ++s) chebyshev<T>(c, L, b, x, false, o);
+      chebyshev<T>(c, L, b, x, true);
+      for (int s = 1; s < o.coarse_sweeps; ++s) {
+        DP_CUDA(cudaMemsetAsync(L.r, 0, sizeof(T) * 2 * L.g.nnod, c.stream));
+        chebyshev<T>(c, L, b, x, false);
+      }
     }
     return;
   }
   MGLevel& C = c.mg[l + 1];
-  chebyshev<T>(c, L, b, x, true, o);
-  // residual r = b - A x into L.r
   T* r = (T*)L.r;
-  apply_level<T>(c, L, x, r);
-  k_sub<T><<<tpb(n), 256, 0, c.stream>>>(b, r, n);
-  const int64_t nc = 2 * C.g.nnod;
+  T* t = (T*)L.t;
   T* bc = (T*)C.b;
   T* xc = (T*)C.x;
-  DP_CUDA(cudaMemsetAsync(bc, 0, sizeof(T) * nc, c.stream));
-  k_restrict<T><<<tpb(L.g.nnod), 256, 0, c.stream>>>(r, bc, (int)L.g.A(), (int)L.g.B(), C.g.ncr, (int)C.g.A(),
-                                                       (int)C.g.B(), L.g.pin);
-  k_mask_fixed<T><<<tpb(2 * C.g.B() + 1), 256, 0, c.stream>>>(bc, (int)C.g.A(), (int)C.g.B(), C.g.pin);
+  // pre-smoothing, then restrict the true residual r - A d_last
+  chebyshev<T>(c, L, b, x, true);
+  launch_apply_K_acc<T, T>(L.g, level_K<T>(L), (const T*)L.d, t, c.stream);
+  ++g_klaunch;
+  k_restrict_g<T><<<tpb(C.g.nnod), 256, 0, c.stream>>>(r, t, bc, (int)L.g.A(), (int)L.g.B(), (int)C.g.A(),
+                                                         (int)C.g.B(), C.g.pin);
   DP_LAUNCH_CHECK();
   vcycle<T>(c, l + 1, bc, xc, o);
-  k_prolong_add<T><<<tpb(L.g.nnod), 256, 0, c.stream>>>(xc, x, (int)L.g.A(), (int)L.g.B(), C.g.ncr, (int)C.g.A(),
+  ++g_klaunch;
+  k_prolong_add<T><<<tpb(L.g.nnod), 256, 0, c.stream>>>(xc, x, r, (int)L.g.A(), (int)L.g.B(), C.g.ncr, (int)C.g.A(),
                                                           (int)C.g.B(), L.g.pin);
   DP_LAUNCH_CHECK();
-  chebyshev<T>(c, L, b, x, false, o);
+  chebyshev<T>(c, L, b, x, false);
 }
 
 void mg_apply(Ctx& c, const double* b, double* x, const MGOptions& o) { vcycle<double>(c, 0, b, x, o); }

@@ -4,10 +4,13 @@
 
 namespace dp {
 
+constexpr int kMaxCheb = 8;
+
 struct MGOptions {
   int cheb_degree = 3;      // Chebyshev steps per smoothing (each one A-apply)
   double cheb_lo = 0.15;    // smoothing interval [lo, hi] * lambda_max(D^-1 A)
   double cheb_hi = 1.1;
+  int block_jacobi = 1;     // 1: 2x2 nodal blocks (u_theta, u_r); 0: point Jacobi
   int max_levels = 16;
   int64_t coarse_max = 1024;// largest dense coarsest system
   int coarse_sweeps = 4;    // smoothing sweeps when the coarsest is not dense

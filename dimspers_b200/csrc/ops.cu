@@ -63,11 +63,22 @@ __global__ void __launch_bounds__(128) k_apply_K(const Tm* __restrict__ K, const
 template <typename Tm, typename Tv>
 void launch_apply_K(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
   DP_CUDA(cudaMemsetAsync(y, 0, sizeof(Tv) * 2 * L.nnod, s));
+  ++g_klaunch;
   k_apply_K<Tm, Tv><<<(int)div_up(L.nel, 128), 128, 0, s>>>(K, x, y, (int)L.nel, L.ncr, (int)L.A(), (int)L.B());
   DP_LAUNCH_CHECK();
 }
 template void launch_apply_K<double, double>(const Level&, const double*, const double*, double*, cudaStream_t);
 template void launch_apply_K<float, float>(const Level&, const float*, const float*, float*, cudaStream_t);
+
+// y += K x (the caller has zeroed y, typically inside the preceding vector kernel)
+template <typename Tm, typename Tv>
+void launch_apply_K_acc(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
+  ++g_klaunch;
+  k_apply_K<Tm, Tv><<<(int)div_up(L.nel, 128), 128, 0, s>>>(K, x, y, (int)L.nel, L.ncr, (int)L.A(), (int)L.B());
+  DP_LAUNCH_CHECK();
+}
+template void launch_apply_K_acc<double, double>(const Level&, const double*, const double*, double*, cudaStream_t);
+template void launch_apply_K_acc<float, float>(const Level&, const float*, const float*, float*, cudaStream_t);
 
 // ---- G / G^T ----------------------------------------------------------------
 __device__ inline void element_nodes_dev(int e, int ncr, int A, int B, int nd[6]) {
@@ -139,6 +150,7 @@ __global__ void k_apply_GT(const double* __restrict__ G, const double* __restric
 void launch_apply_G(Ctx& c, const double* p, double* y) {
   const Level& L = c.fine;
   DP_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * 2 * L.nnod, c.stream));
+  ++g_klaunch;
   k_apply_G<<<(int)div_up(L.nel, 128), 128, 0, c.stream>>>(c.Gp, p, y, (int)L.nel, L.ncr, L.nct, (int)L.A(),
                                                            (int)L.B(), c.mesh.pressure);
   DP_LAUNCH_CHECK();
@@ -147,6 +159,7 @@ void launch_apply_G(Ctx& c, const double* p, double* y) {
 void launch_apply_GT(Ctx& c, const double* x, double* p) {
   const Level& L = c.fine;
   if (c.mesh.pressure == 0) DP_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * c.mesh.npres, c.stream));
+  ++g_klaunch;
   k_apply_GT<<<(int)div_up(L.nel, 128), 128, 0, c.stream>>>(c.Gp, x, p, (int)L.nel, L.ncr, L.nct, (int)L.A(),
                                                             (int)L.B(), c.mesh.pressure);
   DP_LAUNCH_CHECK();
@@ -177,14 +190,17 @@ __global__ void __launch_bounds__(kRedThreads) k_sum(const double* __restrict__ 
 static int red_blocks(int64_t n) { return red_grid(n); }
 
 void launch_dot(Ctx& c, const double* a, const double* b, int64_t n, int slot) {
+  ++g_klaunch;
   k_dot<double><<<red_blocks(n), kRedThreads, 0, c.stream>>>(a, b, n, c.partial, c.counter, c.scal + slot);
   DP_LAUNCH_CHECK();
 }
 void launch_dot_f(Ctx& c, const float* a, const float* b, int64_t n, int slot) {
+  ++g_klaunch;
   k_dot<float><<<red_blocks(n), kRedThreads, 0, c.stream>>>(a, b, n, c.partial, c.counter, c.scal + slot);
   DP_LAUNCH_CHECK();
 }
 void launch_sum(Ctx& c, const double* a, int64_t n, int slot) {
+  ++g_klaunch;
   k_sum<<<red_blocks(n), kRedThreads, 0, c.stream>>>(a, n, c.partial, c.counter, c.scal + slot);
   DP_LAUNCH_CHECK();
 }
@@ -206,11 +222,13 @@ __global__ void k_scatter_lat2ref(const int64_t* __restrict__ ref2lat, const dou
 }
 void launch_gather_ref2lat(Ctx& c, const double* ref, double* lat, int comps) {
   const int64_t n = c.fine.nnod;
+  ++g_klaunch;
   k_gather_ref2lat<<<(int)div_up(n, 256), 256, 0, c.stream>>>(c.ref2lat, ref, lat, n, comps);
   DP_LAUNCH_CHECK();
 }
 void launch_scatter_lat2ref(Ctx& c, const double* lat, double* ref, int comps) {
   const int64_t n = c.fine.nnod;
+  ++g_klaunch;
   k_scatter_lat2ref<<<(int)div_up(n, 256), 256, 0, c.stream>>>(c.ref2lat, lat, ref, n, comps);
   DP_LAUNCH_CHECK();
 }
@@ -220,6 +238,7 @@ __global__ void k_pc_invert(double* pc, int64_t n) {
   if (i < n) pc[i] = 1.0 / pc[i];
 }
 void launch_pc_invert(Ctx& c, double* pc, int64_t n) {
+  ++g_klaunch;
   k_pc_invert<<<(int)div_up(n, 256), 256, 0, c.stream>>>(pc, n);
   DP_LAUNCH_CHECK();
 }

@@ -92,6 +92,47 @@ __global__ void __launch_bounds__(kRedThreads) k_schur_center(double* __restrict
   grid_finish<2>(v, partial, counter, o);
 }
 
+// Element-block mass preconditioner (discontinuous pressure): d_e = M_e^-1 r_e.
+__global__ void k_mass_blk(const double* __restrict__ r, const double* __restrict__ Minv, double* __restrict__ d,
+                           int nel) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nel) return;
+  const double r0 = r[3 * (size_t)e], r1 = r[3 * (size_t)e + 1], r2 = r[3 * (size_t)e + 2];
+  const double a = Minv[e], b = Minv[nel + e], c = Minv[2 * (size_t)nel + e];
+  const double dd = Minv[3 * (size_t)nel + e], f = Minv[4 * (size_t)nel + e], g = Minv[5 * (size_t)nel + e];
+  d[3 * (size_t)e] = a * r0 + b * r1 + c * r2;
+  d[3 * (size_t)e + 1] = b * r0 + dd * r1 + f * r2;
+  d[3 * (size_t)e + 2] = c * r0 + f * r1 + g * r2;
+}
+
+// k_schur_center with d = M^-1 r per element block
+__global__ void __launch_bounds__(kRedThreads) k_schur_center_blk(double* __restrict__ r, const double* __restrict__ rlast,
+                                                                   const double* __restrict__ Minv, double* __restrict__ d,
+                                                                   int nel, double* scal, double* partial,
+                                                                   unsigned int* counter) {
+  const double m = scal[S_SUMR] / (3.0 * (double)nel);
+  double s0 = 0.0, s1 = 0.0;
+  for (int e = blockIdx.x * kRedThreads + threadIdx.x; e < nel; e += gridDim.x * kRedThreads) {
+    double rv[3];
+    for (int k = 0; k < 3; ++k) {
+      rv[k] = r[3 * (size_t)e + k] - m;
+      r[3 * (size_t)e + k] = rv[k];
+    }
+    const double a = Minv[e], b = Minv[nel + e], c = Minv[2 * (size_t)nel + e];
+    const double dd = Minv[3 * (size_t)nel + e], f = Minv[4 * (size_t)nel + e], g = Minv[5 * (size_t)nel + e];
+    const double dv[3] = {a * rv[0] + b * rv[1] + c * rv[2], b * rv[0] + dd * rv[1] + f * rv[2],
+                          c * rv[0] + f * rv[1] + g * rv[2]};
+    for (int k = 0; k < 3; ++k) {
+      d[3 * (size_t)e + k] = dv[k];
+      s0 += rv[k] * rv[k];
+      s1 += (rv[k] - rlast[3 * (size_t)e + k]) * dv[k];
+    }
+  }
+  double v[2] = {s0, s1};
+  double* o[2] = {scal + S_RR, scal + S_BNUM};
+  grid_finish<2>(v, partial, counter, o);
+}
+
 // q = d + beta q, beta = BNUM / RD; sum(q) -> S_SUMQ (for the next rm0space!)
 __global__ void __launch_bounds__(kRedThreads) k_q_update(double* __restrict__ q, const double* __restrict__ d, int64_t n,
                                                            double* scal, double* partial, unsigned int* counter) {
@@ -164,10 +205,19 @@ __global__ void k_pcg_dir(T* __restrict__ p, const T* __restrict__ z, int64_t n,
   if (i < n) p[i] = (T)((double)z[i] + beta * (double)p[i]);
 }
 
-template <typename T>
-__global__ void k_jacobi(const T* __restrict__ dinv, const T* __restrict__ r, T* __restrict__ z, int64_t n) {
+
+__global__ void k_f32_to_f64(const float* __restrict__ a, double* __restrict__ b, int64_t n) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < n) z[i] = dinv[i] * r[i];
+  if (i < n) b[i] = (double)a[i];
+}
+__global__ void k_bj_host_mixed(const float* __restrict__ dinv, const double* __restrict__ r, double* __restrict__ z,
+                                int64_t nnod) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nnod) return;
+  double z0, z1;
+  bj_apply<float>(dinv, n, r[2 * n], r[2 * n + 1], z0, z1);
+  z[2 * n] = z0;
+  z[2 * n + 1] = z1;
 }
 
 template <typename T>
@@ -220,11 +270,27 @@ static int pcg(Ctx& c, const T* Kmat, const T* b, T* x, T* r, T* z, T* p, T* Ap,
   const double tol2 = rtol * rtol * bb;
   auto precond = [&](const T* rin, T* zout) {
     if (pc_kind == 0) {
-      if (std::is_same<T, double>::value) mg_apply(c, (const double*)rin, (double*)zout, mgo);
-      else mg_apply_f(c, (const float*)rin, (float*)zout, mgo);
+      if (std::is_same<T, double>::value && c.mg_prec == 1) {
+        // FP64 vectors, FP32 hierarchy: unscaled conversion (host loop is a debugging path)
+        float* r32 = (float*)c.work[W_F_R];
+        float* z32 = (float*)c.work[W_F_Z];
+        ++g_klaunch;
+        k_scale_copy<float><<<nb256(n), 256, 0, c.stream>>>((const double*)rin, r32, 1.0, n);
+        mg_apply_f(c, r32, z32, mgo);
+        ++g_klaunch;
+        k_f32_to_f64<<<nb256(n), 256, 0, c.stream>>>(z32, (double*)zout, n);
+      } else if (std::is_same<T, double>::value) {
+        mg_apply(c, (const double*)rin, (double*)zout, mgo);
+      } else {
+        mg_apply_f(c, (const float*)rin, (float*)zout, mgo);
+      }
+    } else if (c.mg_prec == 1 && std::is_same<T, double>::value) {
+      ++g_klaunch;
+      k_bj_host_mixed<<<nb256(L.nnod), 256, 0, c.stream>>>(c.mg[0].dinv32, (const double*)rin, (double*)zout, L.nnod);
     } else {
       const T* dinv = std::is_same<T, double>::value ? (const T*)c.mg[0].dinv64 : (const T*)c.mg[0].dinv32;
-      k_jacobi<T><<<nb256(n), 256, 0, c.stream>>>(dinv, rin, zout, n);
+      ++g_klaunch;
+      k_bj<T><<<nb256(L.nnod), 256, 0, c.stream>>>(dinv, rin, zout, L.nnod);
     }
   };
   precond(r, z);
@@ -237,6 +303,7 @@ static int pcg(Ctx& c, const T* Kmat, const T* b, T* x, T* r, T* z, T* p, T* Ap,
     const int nxt = (it & 1) ? S_RZ1 : S_RZ0;
     launch_apply_K<T, T>(L, Kmat, p, Ap, c.stream);
     dot_t<T>(c, p, Ap, n, S_PAP);
+    ++g_klaunch;
     k_pcg_update<T><<<red_grid(n), kRedThreads, 0, c.stream>>>(x, r, p, Ap, n, c.scal, cur, c.partial, c.counter);
     DP_LAUNCH_CHECK();
     rr = read_slot(c, S_IRR);
@@ -244,6 +311,7 @@ static int pcg(Ctx& c, const T* Kmat, const T* b, T* x, T* r, T* z, T* p, T* Ap,
     if (rr <= tol2) break;
     precond(r, z);
     dot_t<T>(c, r, z, n, nxt);
+    ++g_klaunch;
     k_pcg_dir<T><<<nb256(n), 256, 0, c.stream>>>(p, z, n, c.scal, nxt, cur);
     DP_LAUNCH_CHECK();
   }
@@ -259,7 +327,7 @@ int inner_solve(Ctx& c, const double* y, double* z, const SolveCfg& cfg, InnerSt
   double* wz = (double*)c.work[W_IN_Z];
   double* wp = (double*)c.work[W_IN_P];
   double* wAp = (double*)c.work[W_IN_AP];
-  if (cfg.precision == 0) {
+  if (cfg.precision <= 1) {
     double rel = 0.0;
     const int its = pcg<double>(c, c.K64, y, z, w, wz, wp, wAp, cfg.inner_rtol, cfg.inner_itmax, cfg.inner_pc, cfg.mg,
                                 &rel);
@@ -284,12 +352,15 @@ int inner_solve(Ctx& c, const double* y, double* z, const SolveCfg& cfg, InnerSt
   int total = 0;
   for (int ref = 0; ref < cfg.max_refine; ++ref) {
     const double s = std::sqrt(rel * rel * yy);
+    ++g_klaunch;
     k_scale_copy<float><<<nb256(n), 256, 0, c.stream>>>(res, fb, 1.0 / s, n);
     double rel32 = 0.0;
     total += pcg<float>(c, c.K32, fb, fx, fr, fz, fp, fAp, cfg.inner_rtol32, cfg.inner_itmax, cfg.inner_pc, cfg.mg,
                         &rel32);
+    ++g_klaunch;
     k_add_scaled<float><<<nb256(n), 256, 0, c.stream>>>(z, fx, s, n);
     launch_apply_K<double, double>(L, c.K64, z, res, c.stream);
+    ++g_klaunch;
     k_residual<<<nb256(n), 256, 0, c.stream>>>(y, res, n);
     DP_LAUNCH_CHECK();
     launch_dot(c, res, res, n, S_TMP);
@@ -374,21 +445,30 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
   // Rhs = F + G P ; U = K^-1 Rhs   (IterativeSolvers.jl:101-111)
   if (!cfg.use_guess) DP_CUDA(cudaMemsetAsync(P, 0, sizeof(double) * nP, c.stream));
   launch_apply_G(c, P, y);
+  ++g_klaunch;
   k_add<<<nb256(nU), 256, 0, c.stream>>>(c.F, y, rhs, nU);
   DP_LAUNCH_CHECK();
   inner_solve(c, rhs, U, cfg, st);
   // r = -G^T U; rm0space!(r)
   launch_apply_GT(c, U, r);
+  ++g_klaunch;
   k_neg<<<nb256(nP), 256, 0, c.stream>>>(r, nP);
   launch_sum(c, r, nP, S_SUMR);
+  ++g_klaunch;
   k_sub_mean<<<nb256(nP), 256, 0, c.stream>>>(r, nP, c.scal + S_SUMR);
   launch_dot(c, r, r, nP, S_RR);
   DP_LAUNCH_CHECK();
   const double r0 = std::sqrt(read_slot(c, S_RR));
   res.r0 = r0;
   const double tol = r0 * cfg.rtol;
-  // d = r .* pc; q = d
-  k_mul_into<<<nb256(nP), 256, 0, c.stream>>>(r, c.pc, d, nP);
+  // d = r .* pc (or M^-1 r); q = d
+  if (cfg.schur_pc == 1) {
+    ++g_klaunch;
+    k_mass_blk<<<nb256(L.nel), 256, 0, c.stream>>>(r, c.Minv, d, (int)L.nel);
+  } else {
+    ++g_klaunch;
+    k_mul_into<<<nb256(nP), 256, 0, c.stream>>>(r, c.pc, d, nP);
+  }
   DP_CUDA(cudaMemcpyAsync(q, d, sizeof(double) * nP, cudaMemcpyDeviceToDevice, c.stream));
   launch_sum(c, q, nP, S_SUMQ);
   res.status = 1;  // not converged until shown otherwise
@@ -397,6 +477,7 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
   if (r0 == 0.0) res.status = 0;
   for (int it = 1; it <= cfg.itmax && r0 > 0.0; ++it) {
     // rm0space!(q); rd = r.d
+    ++g_klaunch;
     k_q_center_rd<<<red_grid(nP), kRedThreads, 0, c.stream>>>(q, r, d, nP, c.scal, c.partial, c.counter);
     // y = G q ; z = K^-1 y ; Sq = G^T z ; qSq
     launch_apply_G(c, q, y);
@@ -404,10 +485,17 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
     launch_apply_GT(c, z, Sq);
     launch_dot(c, q, Sq, nP, S_QSQ);
     // P += alpha q; U += alpha z; r -= alpha Sq
+    ++g_klaunch;
     k_schur_update_p<<<red_grid(nP), kRedThreads, 0, c.stream>>>(P, r, rlast, q, Sq, nP, c.scal, c.partial, c.counter);
+    ++g_klaunch;
     k_axpy_slot<<<nb256(nU), 256, 0, c.stream>>>(U, z, nU, c.scal);
     // rm0space!(r); d = r .* pc; ||r||; (r - rlast).d
-    k_schur_center<<<red_grid(nP), kRedThreads, 0, c.stream>>>(r, rlast, c.pc, d, nP, c.scal, c.partial, c.counter);
+    ++g_klaunch;
+    if (cfg.schur_pc == 1)
+      k_schur_center_blk<<<red_grid(L.nel), kRedThreads, 0, c.stream>>>(r, rlast, c.Minv, d, (int)L.nel, c.scal,
+                                                                         c.partial, c.counter);
+    else
+      k_schur_center<<<red_grid(nP), kRedThreads, 0, c.stream>>>(r, rlast, c.pc, d, nP, c.scal, c.partial, c.counter);
     DP_LAUNCH_CHECK();
     read_slots(c, 0, 6);
     const double qSq = c.h_scal[S_QSQ], rd = c.h_scal[S_RD];
@@ -425,6 +513,7 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
       break;
     }
     // q = d + beta q
+    ++g_klaunch;
     k_q_update<<<red_grid(nP), kRedThreads, 0, c.stream>>>(q, d, nP, c.scal, c.partial, c.counter);
     DP_LAUNCH_CHECK();
   }
@@ -434,7 +523,9 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
   // residual diagnostics on the raw solution: ||K U - F - G P|| / ||F||, ||G^T U||
   launch_apply_K<double, double>(L, c.K64, U, rhs, c.stream);   // rhs <- K U
   launch_apply_G(c, P, y);                                      // y <- G P
+  ++g_klaunch;
   k_add<<<nb256(nU), 256, 0, c.stream>>>(c.F, y, y, nU);        // y <- F + G P
+  ++g_klaunch;
   k_residual<<<nb256(nU), 256, 0, c.stream>>>(y, rhs, nU);      // rhs <- F + G P - K U
   DP_LAUNCH_CHECK();
   launch_dot(c, rhs, rhs, nU, S_TMP);
@@ -443,6 +534,7 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
   res.mom_residual = std::sqrt(c.h_scal[S_TMP] / std::max(c.h_scal[S_TMP2], 1e-300));
   launch_apply_GT(c, U, Sq);
   launch_sum(c, Sq, nP, S_SUMR);
+  ++g_klaunch;
   k_sub_mean<<<nb256(nP), 256, 0, c.stream>>>(Sq, nP, c.scal + S_SUMR);
   launch_dot(c, Sq, Sq, nP, S_TMP);
   res.div_residual = r0 > 0.0 ? std::sqrt(read_slot(c, S_TMP)) / r0 : 0.0;
@@ -450,8 +542,10 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
   // rigid-rotation removal (updatevelocity2)
   res.omega = 0.0;
   if (cfg.remove_rotation) {
+    ++g_klaunch;
     k_rot_integrals<<<red_grid(L.nel), kRedThreads, 0, c.stream>>>(U, c.rho_lat, c.theta_lat, c.r_lat, (int)L.nel, L.ncr,
                                                                    (int)L.A(), (int)L.B(), c.scal, c.partial, c.counter);
+    ++g_klaunch;
     k_rot_remove<<<nb256(L.nnod), 256, 0, c.stream>>>(U, c.r_lat, L.nnod, c.scal);
     DP_LAUNCH_CHECK();
     read_slots(c, S_AM, 2);
@@ -461,6 +555,7 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
 }
 
 void to_cartesian(Ctx& c, const double* U, double* Uc) {
+  ++g_klaunch;
   k_to_cartesian<<<nb256(c.fine.nnod), 256, 0, c.stream>>>(U, c.theta_lat, Uc, c.fine.nnod);
   DP_LAUNCH_CHECK();
 }

@@ -9,7 +9,7 @@ struct SolveCfg {
   double rtol = 1e-8;       // outer (IterativeSolvers.jl:95)
   int itmax = 200;          // outer (:96)
   int itmin = 10;           // outer (:97)
-  int precision = 0;        // 0 FP64, 1 FP32-refined
+  int precision = 0;        // 0 FP64; 1 FP64 Krylov + FP32 hierarchy; 2 FP32 PCG in FP64 refinement
   int inner_pc = 0;         // 0 multigrid, 1 Jacobi
   double inner_rtol = 1e-10;
   double inner_rtol32 = 1e-5;
@@ -18,6 +18,9 @@ struct SolveCfg {
   int remove_rotation = 1;
   int use_guess = 0;
   int verbose = 0;
+  int host_loop = 0;        // 1: host-driven loops (debug); 0: one CUDA graph per solve
+  double inner_relax = 0.0; // > 0: relaxed inner tolerance with this cap
+  int schur_pc = 0;         // 0 lumped mass (StokesPcCG), 1 element-block mass inverse
   MGOptions mg;
 };
 
@@ -30,6 +33,8 @@ struct SolveResult {
   int status = 0;
   int iterations = 0;
   int64_t inner_its = 0;
+  int64_t launches = 0;       // kernels launched by the solve
+  int64_t refinements = 0;    // FP64 refinement steps (FP32-refined path)
   double relres = 0.0, r0 = 0.0, omega = 0.0, div_residual = 0.0, mom_residual = 0.0;
 };
 
@@ -45,5 +50,7 @@ enum Work {
 int inner_solve(Ctx& c, const double* y, double* z, const SolveCfg& cfg, InnerStats& st);
 int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& res);
 void to_cartesian(Ctx& c, const double* U, double* Uc);
+int schur_pcg_graph(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& res);
+void graph_free(Ctx& c);
 
 }  // namespace dp

@@ -243,6 +243,13 @@ class StokesContext:
             self._chk(st)
         return rep.as_dict()
 
+    def profile_kernel(self, which, reps=50, flush_l2=False):
+        """Average ms per launch: 0 FP32 A-apply, 1 FP64 A-apply, 2 V-cycle;
+        flush_l2 times each launch alone after overwriting 256 MB (cold L2)."""
+        ms = C.c_double(0.0)
+        self._chk(lib().dp_profile_kernel(self.h, int(which), int(reps), 1 if flush_l2 else 0, C.byref(ms)))
+        return ms.value
+
     def set_material_device(self, eta_ptr, ld_eta, rho_ptr, g, C6_ptrs=None, ld_C=0):
         fields = (C.c_void_p * 6)(*C6_ptrs) if C6_ptrs is not None else None
         self._chk(lib().dp_set_material(self.h, C.c_void_p(eta_ptr), int(ld_eta), fields, int(ld_C),

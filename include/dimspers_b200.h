@@ -37,7 +37,11 @@ typedef enum {
 } dp_status;
 
 typedef enum { DP_PRESSURE_CONTINUOUS = 0, DP_PRESSURE_DISCONTINUOUS = 1 } dp_pressure_space;
-typedef enum { DP_PREC_FP64 = 0, DP_PREC_FP32_REFINED = 1 } dp_precision;
+/* FP64: all in FP64.  FP32_REFINED: FP32 element matrices and FP32 multigrid
+ * (the bulk of the applies) preconditioning an FP64 Krylov solve whose
+ * residual, updates and dot products stay FP64.  FP32_IR: classic iterative
+ * refinement, an FP32 PCG inside an FP64 residual / correction loop. */
+typedef enum { DP_PREC_FP64 = 0, DP_PREC_FP32_REFINED = 1, DP_PREC_FP32_IR = 2 } dp_precision;
 typedef enum { DP_MEM_HOST = 0, DP_MEM_DEVICE = 1 } dp_memory;
 typedef enum { DP_INNER_MG = 0, DP_INNER_JACOBI = 1 } dp_inner_pc;
 
@@ -70,6 +74,20 @@ typedef struct {
   int32_t cheb_degree;     /* Chebyshev smoothing steps per level             */
   double inner_rtol32;     /* FP32 inner tolerance per refinement step        */
   int32_t max_refine;      /* FP32-refined: refinement steps per inner solve  */
+  int32_t host_loop;       /* 1: drive the loops from the host (debugging);
+                              0: the whole solve is one CUDA graph with
+                              device-side loop control                        */
+  int32_t block_jacobi;    /* smoother: 1 = 2x2 nodal blocks, 0 = point Jacobi */
+  double cheb_lo, cheb_hi; /* Chebyshev interval as fractions of lambda_max  */
+  double inner_relax;      /* > 0: relax the inner tolerance as the outer
+                              residual falls, inner_rtol * ||r0|| / ||r_k||,
+                              capped at this value; 0: fixed inner_rtol       */
+  int32_t coarse_max;      /* largest coarsest-level system solved densely    */
+  int32_t schur_pc;        /* Schur preconditioner: 0 = 1/rowsum(M), the lumped
+                              mass of StokesPcCG (IterativeSolvers.jl:120,238);
+                              1 = M^-1 from the element mass blocks, what the
+                              incomplete LDL^T of StokesPcCG_pardiso (:32,242)
+                              gives for block-diagonal (discontinuous) M      */
 } dp_solve_opts;
 
 typedef struct {
@@ -84,6 +102,8 @@ typedef struct {
   double t_assemble_ms, t_setup_ms, t_solve_ms;
   int32_t fallback_used;       /* learned guess rejected -> zero guess        */
   int32_t mg_levels;
+  int64_t kernel_launches;     /* kernels this library launched for the solve */
+  int64_t refinements;         /* FP64 refinement steps (FP32-refined path)   */
 } dp_solve_report;
 
 typedef struct dp_ctx dp_ctx;
@@ -165,6 +185,14 @@ int dp_apply_GT(dp_ctx* ctx, const double* x, double* p, int32_t mem);
 int dp_get_rhs(dp_ctx* ctx, double* F, double* pc);
 
 void dp_default_opts(dp_solve_opts* opts);
+
+/* Average device time (ms) of one launch of a hot kernel on the context's
+ * stream, from CUDA events, after an assembly: which = 0 fine-level A-apply
+ * FP32, 1 fine-level A-apply FP64, 2 one multigrid V-cycle (precision of the
+ * last solve).  flush_l2 = 0: `reps` back-to-back launches (warm L2);
+ * 1: a 256 MB buffer is overwritten before each launch and each launch is
+ * timed alone (cold L2, DRAM-bound figure). */
+int dp_profile_kernel(dp_ctx* ctx, int32_t which, int32_t reps, int32_t flush_l2, double* ms_per_launch);
 
 #ifdef __cplusplus
 }

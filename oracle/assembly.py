@@ -99,7 +99,7 @@ def element_matrices(th, r, eta_ip, rho_node, e2n, g, C6=None):
     detJ = J_th[:, 0] * J_r[:, 1] - J_th[:, 1] * J_r[:, 0]
     R31, R21 = r[2] - r[0], r[1] - r[0]
     T31, T21 = th[2] - th[0], th[1] - th[0]
-    Kfull = np.zeros((nel, 12, 12))
+    Kp = np.zeros((78, nel))
     Ge = np.zeros((nel, 36))
     Me = np.zeros((nel, 6))
     Fb = np.zeros((nel, 12))
@@ -119,12 +119,7 @@ def element_matrices(th, r, eta_ip, rho_node, e2n, g, C6=None):
         om = r_ip * detJ * w[ip]
         dNdx = ix0[:, None] * dNds[ip, 0][None, :] + ix1[:, None] * dNds[ip, 1][None, :]
         dNdz = iz0[:, None] * dNds[ip, 0][None, :] + iz1[:, None] * dNds[ip, 1][None, :]
-        B = np.zeros((nel, 3, 12))
-        B[:, 0, 0::2] = dNdx
-        B[:, 1, 1::2] = dNdz
-        B[:, 2, 0::2] = dNdz
-        B[:, 2, 1::2] = dNdx
-        Kfull += om[:, None, None] * np.einsum("eai,eab,ebj->eij", B, D[:, ip], B)
+        _fill_K(Kp, D[:, ip], om, dNdx, dNdz)
         # _fill_Gblk! (:812-823)
         for i in range(3):
             t = om * NP[ip, i]
@@ -138,8 +133,31 @@ def element_matrices(th, r, eta_ip, rho_node, e2n, g, C6=None):
         cte = (om * fg)[:, None] * N[ip][None, :]
         Fb[:, 0::2] += s[:, None] * cte
         Fb[:, 1::2] += c[:, None] * cte
-    Ke = Kfull[:, PACK12[:, 0], PACK12[:, 1]].T.copy()
-    return Ke, Ge.T.copy(), Me.T.copy(), Fb.T.copy()
+    return Kp, Ge.T.copy(), Me.T.copy(), Fb.T.copy()
+
+
+def _fill_K(Kp, D, om, dx, dz):
+    """One IP of _fill_Kblk! (StokesSolver.jl:744-810, C = 1, no clamp): the
+    78 packed entries in the reference's loop order, vectorised over elements.
+    D (nel, 3, 3) already includes eta; isotropic D gives :688-742."""
+    e11, e13, e15 = D[:, 0, 0], D[:, 0, 1], D[:, 0, 2]
+    e33, e35, e55 = D[:, 1, 1], D[:, 1, 2], D[:, 2, 2]
+    idx = 0
+    for i in range(6):
+        xi, zi = dx[:, i], dz[:, i]
+        for j in range(i, 6):
+            xj, zj = dx[:, j], dz[:, j]
+            Kp[idx] += om * (xi * (e11 * xj + e15 * zj) + zi * (e15 * xj + e55 * zj))
+            idx += 1
+            Kp[idx] += om * (xi * (e13 * zj + e15 * xj) + zi * (e35 * zj + e55 * xj))
+            idx += 1
+        for j in range(i, 6):
+            xj, zj = dx[:, j], dz[:, j]
+            if j > i:
+                Kp[idx] += om * (xi * (e15 * xj + e55 * zj) + zi * (e13 * xj + e35 * zj))
+                idx += 1
+            Kp[idx] += om * (xi * (e35 * zj + e55 * xj) + zi * (e33 * zj + e35 * xj))
+            idx += 1
 
 
 def el2dof(e2n):

@@ -43,8 +43,14 @@ def lumped_pc(MM):
     return 1.0 / np.asarray(Ms.sum(axis=1)).ravel()
 
 
-def stokes_pcg(KK, MM, GG, Rhs, ifree, rtol=1e-8, itmax=200, itmin=10, permc="MMD_AT_PLUS_A"):
-    """StokesPcCG (IterativeSolvers.jl:94-168); returns U, P, report."""
+def stokes_pcg(KK, MM, GG, Rhs, ifree, rtol=1e-8, itmax=200, itmin=10, permc="MMD_AT_PLUS_A",
+               schur_pc="lumped"):
+    """StokesPcCG (IterativeSolvers.jl:94-168); returns U, P, report.
+
+    schur_pc="lumped" is the reference's StokesPcCG (:jacobi -> 1/rowsum M);
+    "mass" applies M^-1 with a direct factorisation of the symmetrised M, the
+    `d = pc \\ r` of StokesPcCG_pardiso (:32-34, :82) whose incomplete LDL^T
+    (lldl) is exact for block-diagonal M (discontinuous pressure)."""
     nU = Rhs.size
     U = np.zeros(nU)
     P = np.zeros(GG.shape[1])
@@ -56,8 +62,13 @@ def stokes_pcg(KK, MM, GG, Rhs, ifree, rtol=1e-8, itmax=200, itmin=10, permc="MM
     GT = GG.T.tocsr()
     r = rm0space(-(GT @ U))
     tol = np.sqrt(r @ r) * rtol
-    pc = lumped_pc(MM)
-    d = r * pc
+    if schur_pc == "lumped":
+        pc = lumped_pc(MM)
+        prec = lambda v: v * pc  # noqa: E731
+    else:
+        Mlu = spla.splu((MM + sp.tril(MM, -1).T).tocsc())
+        prec = Mlu.solve
+    d = prec(r)
     q = d.copy()
     rep = PcgReport()
     for it in range(1, itmax + 1):
@@ -78,7 +89,7 @@ def stokes_pcg(KK, MM, GG, Rhs, ifree, rtol=1e-8, itmax=200, itmin=10, permc="MM
         rep.iterations = it
         if nr < tol and it >= itmin:
             break
-        d = r * pc
+        d = prec(r)
         beta = ((r - rlast) @ d) / rd
         q = d + beta * q
     rep.relres = rep.history[-1] / (tol / rtol) if tol > 0 else 0.0
@@ -144,10 +155,11 @@ def assemble(prob, eta_ip, rho_node, g, C6=None):
 
 
 def solve_stokes(prob, eta_ip, rho_node, g, C6=None, rtol=1e-8, itmax=200, itmin=10,
-                 remove_rotation=True):
+                 remove_rotation=True, schur_pc="lumped"):
     """solveStokes (StokesSolver.jl:7-54), solver=:suitesparse."""
     A = assemble(prob, eta_ip, rho_node, g, C6)
-    U, P, rep = stokes_pcg(A["KK"], A["MM"], A["GG"], A["F"], prob.ifree, rtol, itmax, itmin)
+    U, P, rep = stokes_pcg(A["KK"], A["MM"], A["GG"], A["F"], prob.ifree, rtol, itmax, itmin,
+                           schur_pc=schur_pc)
     Upol = U
     om = 0.0
     if remove_rotation:

@@ -115,17 +115,36 @@ def test_solve_reference_tolerance_iterations():
     assert rel(P, ref["P"]) < 1e-6
 
 
-@pytest.mark.parametrize("pressure", ["continuous", "discontinuous"])
-def test_solve_fp32_refined(pressure):
+@pytest.mark.parametrize("pressure,precision", [("continuous", 1), ("discontinuous", 1),
+                                                ("continuous", 2), ("discontinuous", 2)])
+def test_solve_fp32_refined(pressure, precision):
+    """FP32 element matrices / FP32 multigrid with FP64 residuals (precision 1)
+    and classic FP32 iterative refinement (precision 2) against the FP64 oracle."""
     prob, mat, ctx = _setup(8, 64, pressure, "aniso")
     ref = OS.solve_stokes(prob, mat.eta_ip, mat.rho, mat.g, mat.C6, rtol=1e-12, itmax=5000)
     with ctx:
         ctx.set_material(mat.eta_ip, mat.rho, mat.g, mat.C6)
-        ctx.assemble(1)
-        U, P, Uc, rep = ctx.solve(precision=1, rtol=1e-11, itmax=5000, inner_rtol=1e-12)
+        ctx.assemble(precision)
+        U, P, Uc, rep = ctx.solve(precision=precision, rtol=1e-11, itmax=5000, inner_rtol=1e-12)
     assert rep["status"] == 0, rep
     assert rel(U, ref["U"]) < 1e-7, rel(U, ref["U"])
     assert rel(P, ref["P"]) < 1e-7, rel(P, ref["P"])
+
+
+@pytest.mark.parametrize("precision", [0, 1, 2])
+def test_graph_matches_host_loop(precision):
+    """The single-graph solve (device-side loop control) and the host-driven
+    loops run the same kernels in the same order."""
+    prob, mat, ctx = _setup(8, 64, "discontinuous", "aniso")
+    with ctx:
+        ctx.set_material(mat.eta_ip, mat.rho, mat.g, mat.C6)
+        ctx.assemble(precision)
+        U0, P0, _, r0 = ctx.solve(precision=precision, host_loop=1, itmax=5000, rtol=1e-11, inner_rtol=1e-12)
+        U1, P1, _, r1 = ctx.solve(precision=precision, itmax=5000, rtol=1e-11, inner_rtol=1e-12)
+    assert r0["status"] == 0 and r1["status"] == 0
+    assert abs(r0["iterations"] - r1["iterations"]) <= max(3, r0["iterations"] // 50)
+    assert rel(U1, U0) < 1e-7 and rel(P1, P0) < 1e-7
+    assert r1["kernel_launches"] > 0
 
 
 def test_jacobi_inner_matches_mg():
@@ -151,3 +170,36 @@ def test_fse_director_kernel():
     vmax = v[:, :, 1]
     # sign is arbitrary: compare the projector
     assert np.allclose(np.abs(dx * vmax[:, 0] + dy * vmax[:, 1]), 1.0, atol=1e-10)
+
+
+def test_mass_schur_preconditioner_matches_oracle():
+    """schur_pc = 1 (element-block M^-1, discontinuous pressure) against the
+    oracle's StokesPcCG with the same preconditioner: same solution, fewer
+    outer iterations than the lumped mass."""
+    prob, mat, ctx = _setup(8, 64, "discontinuous", "aniso")
+    ref = OS.solve_stokes(prob, mat.eta_ip, mat.rho, mat.g, mat.C6, rtol=1e-12, itmax=5000, schur_pc="mass")
+    ref8 = OS.solve_stokes(prob, mat.eta_ip, mat.rho, mat.g, mat.C6, rtol=1e-8, itmax=5000, schur_pc="mass")
+    with ctx:
+        ctx.set_material(mat.eta_ip, mat.rho, mat.g, mat.C6)
+        ctx.assemble(1)
+        U, P, _, rep = ctx.solve(precision=1, schur_pc=1, rtol=1e-12, itmax=5000, inner_rtol=1e-13)
+        _, _, _, rep8 = ctx.solve(precision=1, schur_pc=1, rtol=1e-8, itmax=5000, inner_rtol=1e-12)
+        _, _, _, rep_l = ctx.solve(precision=1, schur_pc=0, rtol=1e-8, itmax=5000, inner_rtol=1e-12)
+    assert rep["status"] == 0
+    assert rel(U, ref["U"]) < 1e-8 and rel(P, ref["P"]) < 1e-8
+    assert abs(rep8["iterations"] - ref8["report"].iterations) <= 3
+    assert rep8["iterations"] < 0.8 * rep_l["iterations"]
+
+
+def test_relaxed_inner_tolerance_accuracy():
+    """The relaxed inner tolerance keeps U, P within 1e-7 of the fixed-tolerance
+    solve on a well-conditioned (Taylor-Hood) case while doing less inner work."""
+    prob, mat, ctx = _setup(32, 256, "continuous", "aniso")
+    with ctx:
+        ctx.set_material(mat.eta_ip, mat.rho, mat.g, mat.C6)
+        ctx.assemble(1)
+        U0, P0, _, r0 = ctx.solve(precision=1, inner_rtol=1e-12)
+        U1, P1, _, r1 = ctx.solve(precision=1, inner_rtol=1e-10, inner_relax=1e-6)
+    assert r1["status"] == 0
+    assert rel(U1, U0) < 1e-7 and rel(P1, P0) < 1e-7
+    assert r1["inner_iterations"] < r0["inner_iterations"]
