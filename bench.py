@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-iters", type=int, default=3)
     ap.add_argument("--cpu-sample-only", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--host-loop", action="store_true",
+                    help="drive the solver loops from the host (same kernels, one launch each; for ncu launch lists,"
+                         " which cannot see inside graphs with conditional nodes)")
     ap.add_argument("--profile-apply", action="store_true",
                     help="assemble the workload and launch the fine-level FP32 A-apply 3 times (for ncu)")
     return ap.parse_args()
@@ -205,7 +208,7 @@ def run_ours(args, rank, world, local):
     P_d = torch.zeros(npres, dtype=torch.float64, device=dev)
     torch.cuda.synchronize()
 
-    opts = dict(rtol=args.rtol, itmax=args.itmax, itmin=10)
+    opts = dict(rtol=args.rtol, itmax=args.itmax, itmin=10, host_loop=1 if args.host_loop else 0)
     if args.pressure != "discontinuous":
         FAST["schur_pc"] = 0
 

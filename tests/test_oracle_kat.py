@@ -1,0 +1,130 @@
+"""Known-answer tests that pin the FP64 oracle (CPU, no GPU).
+
+The reference has no tests, fixtures or golden vectors, and Julia is absent,
+so the oracle is pinned by properties its algorithm must satisfy exactly (or to
+rounding) plus regression fixtures in tests/golden/ (make_golden.py).
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, MeshView, rel
+from dimspers_b200 import inputs
+from oracle import assembly as OA
+from oracle import mesh as OM
+from oracle import quadrature as OQ
+from oracle import solver as OS
+
+GOLD = os.path.join(ROOT, "tests", "golden")
+
+
+def test_six_point_rule_is_degree_four_exact():
+    """ip_triangle6 (Quadrature.jl:80-107) integrates r^a s^b, a+b <= 4, exactly:
+    int_T r^a s^b = a! b! / (a+b+2)!."""
+    x, w = OQ.ip_triangle6()
+    for a in range(5):
+        for b in range(5 - a):
+            exact = math.factorial(a) * math.factorial(b) / math.factorial(a + b + 2)
+            assert abs(np.sum(w * x[:, 0] ** a * x[:, 1] ** b) - exact) < 1e-15
+
+
+def test_p2_shape_functions():
+    nodes = [(0, 0), (1, 0), (0, 1), (0.5, 0), (0.5, 0.5), (0, 0.5)]
+    for k, p in enumerate(nodes):
+        N = OQ.sf_N_tri6(*p)
+        assert np.allclose(N, np.eye(6)[k], atol=1e-15)
+    for p in [(0.2, 0.3), (0.7, 0.1)]:
+        assert abs(OQ.sf_N_tri6(*p).sum() - 1) < 1e-15
+        assert np.allclose(OQ.sf_dN_tri6(*p).sum(axis=1), 0, atol=1e-14)
+
+
+def test_volume_integral_is_annulus_area():
+    """volume_integral(1) (FSE.jl:412-464) = pi (r_out^2 - r_in^2): the
+    integrand r is linear in (theta, r) and the geometry is exact there."""
+    prob = OS.make_problem(4, 32)
+    area = OS.volume_integral(np.ones(prob.gr.nnod), prob.gr.e2n, prob.th, prob.r)
+    assert abs(area - math.pi * (2.22 ** 2 - 1.22 ** 2)) < 1e-12
+
+
+def test_literal_and_vectorised_edge_numbering_agree():
+    for ncr, nct in [(3, 7), (4, 32)]:
+        a = OM.grid_cells(ncr, nct, literal=True)
+        b = OM.grid_cells(ncr, nct, literal=False)
+        assert np.array_equal(a.e2n, b.e2n) and np.array_equal(a.theta, b.theta)
+
+
+def test_colouring_valid():
+    g = OM.grid_cells(8, 64)
+    colors, lists = OM.color_mesh(g.e2n)
+    for ids in lists:
+        nodes = g.e2n[:3, ids].ravel()
+        assert np.unique(nodes).size == nodes.size
+
+
+@pytest.mark.parametrize("kind", ["iso", "aniso", "fabric"])
+def test_element_matrices_symmetric_psd_translation_null(kind):
+    prob = OS.make_problem(4, 32)
+    mat = inputs.make_material(MeshView(prob), kind, seed=5)
+    Ke, Ge, Me, Fb = OA.element_matrices(prob.th, prob.r, mat.eta_ip, mat.rho, prob.gr.e2n, mat.g, mat.C6)
+    full = OA.unpack_sym(Ke, 12, OA.PACK12)
+    ev = np.linalg.eigvalsh(full)
+    assert ev.min() > -1e-12 * ev.max()
+    # Cartesian rigid translations are exactly in the kernel
+    t1 = np.zeros(12); t1[0::2] = 1
+    t2 = np.zeros(12); t2[1::2] = 1
+    scale = np.abs(full).max()
+    assert np.abs(full @ t1).max() < 1e-13 * scale and np.abs(full @ t2).max() < 1e-13 * scale
+    # two exact zero modes per element: the Cartesian translations (the small
+    # rotation (-z, x) is not in P2 on the (theta, r)-mapped element)
+    assert np.sum(ev < 1e-12 * ev.max(axis=1, keepdims=True)) >= 2 * prob.gr.nel
+
+
+def test_isotropic_tensor_is_rotation_invariant():
+    """directRotation2D (anisotropy.jl:503-536) with e = (a-h)/2 = 1 leaves the
+    isotropic tensor unchanged for any director."""
+    phi = np.linspace(0, 2 * np.pi, 17)
+    C = inputs.ti_tensor(np.ones_like(phi), np.cos(phi), np.sin(phi))
+    ref = (4 / 3, 4 / 3, 1.0, -2 / 3, 0.0, 0.0)
+    for c, r in zip(C, ref):
+        assert np.allclose(c, r, atol=1e-14)
+
+
+def test_rotation_matrix_orthogonal():
+    g = OM.grid_cells(2, 8)
+    TT = OA.rotation_matrix(g.theta).toarray()
+    assert np.allclose(TT @ TT.T, np.eye(TT.shape[0]), atol=1e-14)
+
+
+def test_solution_has_the_forcing_symmetry():
+    """Iso material and forcing with 4-fold symmetry (no noise): the converged
+    velocity is invariant under a rotation by pi/2 (node permutation)."""
+    prob = OS.make_problem(4, 32, "continuous", pin_rotation=False)
+    g = prob.gr
+    T = np.log(g.r / 2.22) / np.log(1.22 / 2.22) + 0.01 * np.cos(4 * g.theta) * np.sin(np.pi * (g.r - 1.22))
+    eta = inputs.eta_from_T(T, g.e2n, 1e3)
+    out = OS.solve_stokes(prob, eta, T, 1e5, rtol=1e-12, itmax=2000)
+    U = out["U"]
+    key = {(round(t, 9) % round(2 * np.pi, 9), round(r, 9)): i for i, (t, r) in enumerate(zip(g.theta, g.r))}
+    perm = np.array([key[(round((t + np.pi / 2) % (2 * np.pi), 9) % round(2 * np.pi, 9), round(r, 9))]
+                     for t, r in zip(g.theta, g.r)])
+    assert rel(U[0::2][perm], U[0::2]) < 1e-6
+    assert rel(U[1::2][perm], U[1::2]) < 1e-6
+
+
+@pytest.mark.parametrize("name", ["iso_4x32_cont", "aniso_4x32_disc", "aniso_8x64_disc_mass", "fabric_8x64_cont"])
+def test_oracle_reproduces_golden(name):
+    meta = json.load(open(os.path.join(GOLD, "golden.json")))[name]
+    gold = np.load(os.path.join(GOLD, name + ".npz"))
+    prob = OS.make_problem(meta["nr_cells"], meta["ntheta_cells"], meta["pressure"], pin_rotation=True)
+    mat = inputs.make_material(MeshView(prob), meta["kind"], seed=meta["seed"])
+    out = OS.solve_stokes(prob, mat.eta_ip, mat.rho, mat.g, mat.C6, rtol=1e-12, itmax=5000,
+                          schur_pc=meta["schur_pc"])
+    tol = 1e-10 if meta["pressure"] == "continuous" else 1e-8
+    assert rel(out["U"], gold["U"]) < tol and rel(out["P"], gold["P"]) < tol
+    assert abs(out["report"].iterations - meta["iterations_rtol12"]) <= 2
+    assert rel(out["mats"]["F"], gold["F"]) < 1e-14
+    import hashlib
+    assert hashlib.sha256(np.ascontiguousarray(prob.gr.e2n).tobytes()).hexdigest() == meta["e2n_sha256"]
