@@ -7,3 +7,4 @@
 #include "solver.cu"
 #include "graph.cu"
 #include "capi.cu"
+#include "noalloc.cu"

@@ -186,6 +186,16 @@ int dp_get_rhs(dp_ctx* ctx, double* F, double* pc);
 
 void dp_default_opts(dp_solve_opts* opts);
 
+/* y = K x like dp_apply_K, for callers that cannot allocate device memory
+ * (inside a stream capture, under an external allocator, after start-up in a
+ * real-time loop).  No counterpart in the reference.  x and y are DEVICE
+ * pointers (2*nnod, reference numbering); the two staging vectors live in one
+ * static 32 MiB device array of the library, so nnod <= 1,048,576 (larger
+ * meshes: DP_BAD_ARG).  No cudaMalloc/cudaFree is called.  All calls on a
+ * device share that array: calls that overlap on the GPU race.  The first call
+ * on a device looks up the array's address; make it before any stream capture. */
+int dp_apply_K_noalloc(dp_ctx* ctx, const double* x, double* y);
+
 /* Average device time (ms) of one launch of a hot kernel on the context's
  * stream, from CUDA events, after an assembly: which = 0 fine-level A-apply
  * FP32, 1 fine-level A-apply FP64, 2 one multigrid V-cycle (precision of the
