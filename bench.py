@@ -62,6 +62,7 @@ def parse():
                     help="drive the solver loops from the host (same kernels, one launch each; for ncu launch lists,"
                          " which cannot see inside graphs with conditional nodes)")
     ap.add_argument("--no-clocks", action="store_true", help="do not sample nvidia-smi (for profiler runs)")
+    ap.add_argument("--no-guess", action="store_true", help="fast arm without the learned initial guess")
     ap.add_argument("--profile-apply", action="store_true",
                     help="assemble the workload and launch the fine-level FP32 A-apply 3 times (for ncu)")
     return ap.parse_args()
@@ -213,11 +214,21 @@ def run_ours(args, rank, world, local):
     if args.pressure != "discontinuous":
         FAST["schur_pc"] = 0
 
+    # learned initial guess (trained weights for this mesh, if present)
+    from dimspers_b200 import learned
+    guess = None
+    wpath = learned.weights_path(args.nr, args.nt)
+    if not args.no_guess and os.path.exists(wpath):
+        guess = learned.LearnedGuess(learned.GuessNet.load(wpath, max_batch=1, device=local), ctx)
+
     def step(precision):
         arm = FAST if precision else PLAIN
         ctx.set_material_ti_device(eta_d.data_ptr(), nel, rho_d.data_ptr(), mat.g, dl_d.data_ptr(),
                                    dx_d.data_ptr(), dy_d.data_ptr())
         ctx.assemble(arm["precision"])
+        if precision and guess is not None:
+            guess.predict(mat.g, P_d.data_ptr())
+            return ctx.solve_device(U_d.data_ptr(), P_d.data_ptr(), None, use_guess=2, **opts, **arm)
         return ctx.solve_device(U_d.data_ptr(), P_d.data_ptr(), None, **opts, **arm)
 
     def barrier():
@@ -275,6 +286,9 @@ def run_ours(args, rank, world, local):
                                           C.c_void_p(rho_h.data_ptr()), float(mat.g), DP_MEM_HOST))
         ctx.assemble(1)
         o = __import__("dimspers_b200").default_opts(**opts, **FAST)
+        if guess is not None:
+            guess.predict(mat.g, P_h.data_ptr(), mem=0)
+            o.use_guess = 2
         rep = SolveReport()
         st = lib().dp_solve(ctx.h, C.c_void_p(U_h.data_ptr()), C.c_void_p(P_h.data_ptr()), None, C.byref(o),
                             C.byref(rep), DP_MEM_HOST)
@@ -332,12 +346,14 @@ def run_ours(args, rank, world, local):
         "config": {"workload": f"annulus {args.nr}x{args.nt} cells, {nel} P2 elements, {2 * nnod} velocity DOF, "
                                f"{npres} {args.pressure} P1 pressure DOF, {args.kind} viscosity",
                    "nr_cells": args.nr, "ntheta_cells": args.nt, "pressure": args.pressure, "material": args.kind,
-                   "rtol": args.rtol, "guess": "zero",
+                   "rtol": args.rtol,
+                   "guess": ("learned (" + os.path.basename(wpath) + ")") if guess is not None else "zero",
                    "fast_arm": FAST, "plain_arm": PLAIN,
                    "parallelism": f"replicas x{world}",
                    "l2": "each step re-assembles > 400 MB of element blocks (L2 is 126 MB); no extra flush"},
         "outer_iterations": last["iterations"], "inner_iterations": last["inner_iterations"],
         "refinements": last["refinements"], "status": last["status"], "relres": last["relres"],
+        "guess_fallback": last["fallback_used"], "r0_guess_over_r0": (last["r0_guess"] / last["r0"]) if guess else None,
         "mom_residual": last["mom_residual"], "mg_levels": last["mg_levels"],
         "fp64": fp64, "fast_vs_fp64": (value / fp64["value"]) if fp64 else None, "fast_vs_fp64_error": err,
         "e2e": {"value": world * args.steps / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,

@@ -39,7 +39,7 @@ class SolveReport(C.Structure):
                 ("div_residual", C.c_double), ("mom_residual", C.c_double),
                 ("t_assemble_ms", C.c_double), ("t_setup_ms", C.c_double), ("t_solve_ms", C.c_double),
                 ("fallback_used", C.c_int32), ("mg_levels", C.c_int32), ("kernel_launches", C.c_int64),
-                ("refinements", C.c_int64)]
+                ("refinements", C.c_int64), ("r0_guess", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -74,6 +74,17 @@ SIGNATURES = {
     "dp_get_rhs": (C.c_int, [_P, _P, _P]),
     "dp_default_opts": (None, [C.POINTER(SolveOpts)]),
     "dp_profile_kernel": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
+    "dp_cnn_create": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, _I32, C.c_int32, C.c_int32,
+                                C.POINTER(_P)]),
+    "dp_cnn_destroy": (None, [_P]),
+    "dp_cnn_num_params": (C.c_int64, [_P]),
+    "dp_cnn_set_params": (C.c_int, [_P, _P, C.c_int64]),
+    "dp_cnn_get_params": (C.c_int, [_P, _P, _P, C.c_int64]),
+    "dp_cnn_forward": (C.c_int, [_P, _P, _P, C.c_int32]),
+    "dp_cnn_gradients": (C.c_int, [_P, _P, _P, C.c_int32, C.POINTER(C.c_double)]),
+    "dp_cnn_train_step": (C.c_int, [_P, _P, _P, C.c_int32, C.c_float, C.POINTER(C.c_double)]),
+    "dp_cnn_inputs": (C.c_int, [_P, _P, C.c_int32, C.c_int32]),
+    "dp_guess_from_grid": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_double, _P, C.c_int32]),
 }
 
 _lib = None

@@ -282,9 +282,9 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs p) {
     }
   }
   if (p.K64)
-    for (int i = 0; i < kKe; ++i) p.K64[(size_t)i * p.nel + e] = ACC(i);
+    for (int i = 0; i < kKe; ++i) p.K64[kidx64(i, e)] = ACC(i);
   if (p.K32)
-    for (int i = 0; i < kKe; ++i) p.K32[(size_t)i * p.nel + e] = (float)ACC(i);
+    for (int i = 0; i < kKe; ++i) p.K32[kidx32(i, e)] = (float)ACC(i);
   // G rows and F: T_k^T applied per node, wall u_r rows zeroed
 #pragma unroll
   for (int k = 0; k < 6; ++k) {

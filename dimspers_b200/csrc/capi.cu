@@ -126,9 +126,13 @@ static SolveCfg make_cfg(const dp_solve_opts* o) {
   return cfg;
 }
 
-__global__ void k_f64_to_f32(const double* a, float* b, int64_t n) {
+// FP32 copy of the packed FP64 element matrices (the layouts differ)
+__global__ void k_f64_to_f32(const double* a, float* b, int64_t nel) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < n) b[i] = (float)a[i];
+  if (i >= nel * kKe) return;
+  const int64_t e = i % nel;
+  const int p = (int)(i / nel);
+  b[kidx32(p, e)] = (float)a[kidx64(p, e)];
 }
 
 }  // namespace dp
@@ -250,7 +254,8 @@ int dp_ctx_create(const dp_mesh_desc* d, dp_ctx** out) {
     dalloc(&c.eta, kNip * nel);
     dalloc(&c.rho_lat, nn);
     dalloc(&c.rho_ref, nn);
-    dalloc(&c.K64, kKe * nel);
+    dalloc(&c.K64, kstore<double>(nel));
+    DP_CUDA(cudaMemset(c.K64, 0, sizeof(double) * kstore<double>(nel)));
     dalloc(&c.Gp, kGe * nel);
     dalloc(&c.F, 2 * nn);
     dalloc(&c.pc, np);
@@ -385,7 +390,10 @@ int dp_assemble(dp_ctx* h, int32_t precision) {
     DP_CUDA(cudaSetDevice(c.device));
     if (c.mat_kind == MAT_NONE) throw BadArg("material not set");
     if (precision < 0 || precision > 2) throw BadArg("precision must be 0, 1 or 2");
-    if (precision >= 1 && !c.K32) dalloc(&c.K32, kKe * c.fine.nel);
+    if (precision >= 1 && !c.K32) {
+      dalloc(&c.K32, kstore<float>(c.fine.nel));
+      DP_CUDA(cudaMemset(c.K32, 0, sizeof(float) * kstore<float>(c.fine.nel)));
+    }
     launch_assemble(c, precision, nullptr);
     c.assembled = precision;
     c.mg_prec = c.mg.empty() ? -1 : c.mg_prec;  // hierarchy values are rebuilt on the next solve
@@ -431,10 +439,13 @@ int dp_solve(dp_ctx* h, double* U, double* P, double* Ucart, const dp_solve_opts
       throw BadArg("schur_pc = 1 (element-block mass inverse) needs discontinuous pressure");
     const int64_t nn = c.fine.nnod, np = c.mesh.npres;
     if (cfg.precision >= 1 && c.assembled == 0) {
-      if (!c.K32) dalloc(&c.K32, kKe * c.fine.nel);
+      if (!c.K32) {
+        dalloc(&c.K32, kstore<float>(c.fine.nel));
+        DP_CUDA(cudaMemsetAsync(c.K32, 0, sizeof(float) * kstore<float>(c.fine.nel), c.stream));
+      }
       const int64_t n = kKe * c.fine.nel;
       ++g_klaunch;
-      k_f64_to_f32<<<(int)div_up(n, 256), 256, 0, c.stream>>>(c.K64, c.K32, n);
+      k_f64_to_f32<<<(int)div_up(n, 256), 256, 0, c.stream>>>(c.K64, c.K32, c.fine.nel);
       DP_LAUNCH_CHECK();
       c.assembled = 1;
     }
@@ -447,6 +458,8 @@ int dp_solve(dp_ctx* h, double* U, double* P, double* Ucart, const dp_solve_opts
     DP_CUDA(cudaEventRecord(e1, c.stream));
     double* dU = (double*)c.work[W_U];
     double* dP = (double*)c.work[W_P];
+    if (cfg.use_guess < 0 || cfg.use_guess > 2) throw BadArg("use_guess must be 0, 1 or 2");
+    if (cfg.use_guess == 2 && cfg.host_loop) throw BadArg("the learned-guess mode runs in the graph path only");
     if (cfg.use_guess) {
       DP_CUDA(cudaMemcpyAsync(dP, P, sizeof(double) * np, kind_in(mem), c.stream));
     }
@@ -491,6 +504,8 @@ int dp_solve(dp_ctx* h, double* U, double* P, double* Ucart, const dp_solve_opts
       rep->mg_levels = (int)c.mg.size();
       rep->kernel_launches = res.launches;
       rep->refinements = res.refinements;
+      rep->fallback_used = res.fallback;
+      rep->r0_guess = res.r0_guess;
     }
     if (res.status == 1) c.err = "outer iteration cap reached";
     if (res.status == 2) c.err = "breakdown: q.Sq <= 0 or non-finite scalar";

@@ -210,4 +210,26 @@ __host__ __device__ constexpr int packed_index12(int R, int C) {
 
 inline int64_t div_up(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Packed element matrices are stored array-of-structures-of-arrays: elements in
+// warp blocks of 32; inside a block the 78 entries of consecutive elements are
+// interleaved in 16-byte groups (2 doubles / 4 floats), so a warp loading group j
+// of its 32 elements reads 512 contiguous bytes and each thread issues 39
+// (FP64) or 20 (FP32, 78 entries padded to 80) 16-byte loads.
+__host__ __device__ inline int64_t kpad(int64_t nel) { return (nel + 31) & ~(int64_t)31; }
+__host__ __device__ inline int64_t kidx64(int p, int64_t e) {
+  return (e >> 5) * (32 * 78) + (int64_t)(p >> 1) * 64 + (e & 31) * 2 + (p & 1);
+}
+__host__ __device__ inline int64_t kidx32(int p, int64_t e) {
+  return (e >> 5) * (32 * 80) + (int64_t)(p >> 2) * 128 + (e & 31) * 4 + (p & 3);
+}
+template <typename T>
+__host__ __device__ inline int64_t kidx(int p, int64_t e);
+template <>
+__host__ __device__ inline int64_t kidx<double>(int p, int64_t e) { return kidx64(p, e); }
+template <>
+__host__ __device__ inline int64_t kidx<float>(int p, int64_t e) { return kidx32(p, e); }
+// number of T in the packed store of nel elements
+template <typename T>
+inline int64_t kstore(int64_t nel) { return kpad(nel) * (sizeof(T) == 8 ? 78 : 80); }
+
 }  // namespace dp

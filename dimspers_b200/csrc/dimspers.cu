@@ -8,3 +8,4 @@
 #include "graph.cu"
 #include "capi.cu"
 #include "noalloc.cu"
+#include "cnn.cu"

@@ -29,14 +29,14 @@ struct DevCtl {
   double rtol, inner_rtol, inner_rtol32, relax_cap;
   int itmax, itmin, inner_itmax, max_refine;
   // state
-  int outer_it, in_it, in32_it, ref_it, status, pad;
+  int outer_it, in_it, in32_it, ref_it, status, guess_used;
   long long in_total, in32_total, ref_total;
-  double r0, tol, in_tol2, in32_tol2, ref_tol2;
+  double r0, tol, in_tol2, in32_tol2, ref_tol2, r0ref, r0guess;
 };
 
 enum GSlot { G_RZ = 16, G_RZN = 17, G_PAP = 18, G_IRR = 19, G_YY = 20,
              F_RZ = 21, F_RZN = 22, F_PAP = 23, F_IRR = 24, F_YY = 25,
-             R_YY = 26, R_RES2 = 27, G_TMP3 = 28 };
+             R_YY = 26, R_RES2 = 27, G_TMP3 = 28, G_RZREF = 29 };
 
 // ---- control kernels (one thread) ---------------------------------------------
 // Inner tolerance: fixed, or (relax) loosened in proportion to the outer
@@ -89,8 +89,11 @@ __global__ void k_ref_check(cudaGraphConditionalHandle h, DevCtl* ctl, const dou
   cudaGraphSetConditional(h, (isfinite(rr) && rr > ctl->ref_tol2 && it < ctl->max_refine) ? 1u : 0u);
 }
 
-__global__ void k_outer_init(cudaGraphConditionalHandle h, DevCtl* ctl, const double* scal) {
-  const double r0 = sqrt(scal[S_RR]);
+// use_ref: the stopping tolerance is relative to the zero-guess residual
+// ||r(P = 0)|| (learned-guess mode), so a guess shortens the solve only by
+// starting closer to the same absolute target.
+__global__ void k_outer_init(cudaGraphConditionalHandle h, DevCtl* ctl, const double* scal, int use_ref) {
+  const double r0 = use_ref ? ctl->r0ref : sqrt(scal[S_RR]);
   ctl->r0 = r0;
   ctl->tol = r0 * ctl->rtol;
   ctl->outer_it = 0;
@@ -112,6 +115,30 @@ __global__ void k_outer_check(cudaGraphConditionalHandle h, DevCtl* ctl, const d
     go = 0u;
   }
   cudaGraphSetConditional(h, go);
+}
+
+// Learned-guess selection: keep the guess only if its initial Schur residual
+// is below the zero guess's (otherwise fall back to P = 0).
+__global__ void k_guess_select(DevCtl* ctl, double* scal) {
+  const double rg = scal[S_RR], rz = scal[G_RZREF];
+  const int use = rg < rz ? 1 : 0;
+  ctl->guess_used = use;
+  ctl->r0ref = sqrt(rz);
+  ctl->r0guess = sqrt(rg);
+  if (!use) {
+    scal[S_RR] = rz;
+  }
+}
+__global__ void k_guess_apply(const DevCtl* ctl, double* __restrict__ U, const double* __restrict__ Uz,
+                              double* __restrict__ r, const double* __restrict__ rz, double* __restrict__ P,
+                              int64_t nU, int64_t nP) {
+  if (ctl->guess_used) return;
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < nU) U[i] = Uz[i];
+  if (i < nP) {
+    r[i] = rz[i];
+    P[i] = 0.0;
+  }
 }
 
 // ---- PCG vector kernels reading their scalars from the table --------------------
@@ -349,6 +376,19 @@ static void emit_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
   double* rhs = (double*)c.work[W_RHS];
   DevCtl* ctl = (DevCtl*)c.ctl;
   DP_CUDA(cudaMemsetAsync(&ctl->in_total, 0, 3 * sizeof(long long), c.stream));
+  if (cfg.use_guess == 2) {
+    // zero-guess reference: Uz = K^-1 F, rz = -G^T Uz (mean removed), ||rz||
+    double* Uz = (double*)c.work[W_UC];
+    double* rz = (double*)c.work[W_RLAST];
+    emit_inner(c, cfg, c.F, Uz, 0, 0);
+    launch_apply_GT(c, Uz, rz);
+    ++g_klaunch;
+    k_neg<<<g_nb(nP), 256, 0, c.stream>>>(rz, nP);
+    launch_sum(c, rz, nP, S_SUMR);
+    ++g_klaunch;
+    k_sub_mean<<<g_nb(nP), 256, 0, c.stream>>>(rz, nP, c.scal + S_SUMR);
+    launch_dot(c, rz, rz, nP, G_RZREF);
+  }
   // Rhs = F + G P ; U = K^-1 Rhs
   if (!cfg.use_guess) DP_CUDA(cudaMemsetAsync(P, 0, sizeof(double) * nP, c.stream));
   launch_apply_G(c, P, y);
@@ -363,6 +403,13 @@ static void emit_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
   ++g_klaunch;
   k_sub_mean<<<g_nb(nP), 256, 0, c.stream>>>(r, nP, c.scal + S_SUMR);
   launch_dot(c, r, r, nP, S_RR);
+  if (cfg.use_guess == 2) {
+    ++g_klaunch;
+    k_guess_select<<<1, 1, 0, c.stream>>>(ctl, c.scal);
+    ++g_klaunch;
+    k_guess_apply<<<g_nb(std::max(nU, nP)), 256, 0, c.stream>>>(ctl, U, (const double*)c.work[W_UC], r,
+                                                                  (const double*)c.work[W_RLAST], P, nU, nP);
+  }
   // d = r .* pc (or M^-1 r) ; q = d
   if (cfg.schur_pc == 1) {
     ++g_klaunch;
@@ -375,7 +422,7 @@ static void emit_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
   launch_sum(c, q, nP, S_SUMQ);
   cudaGraphConditionalHandle h = new_handle(c.stream);
   ++g_klaunch;
-  k_outer_init<<<1, 1, 0, c.stream>>>(h, ctl, c.scal);
+  k_outer_init<<<1, 1, 0, c.stream>>>(h, ctl, c.scal, cfg.use_guess == 2 ? 1 : 0);
   DP_LAUNCH_CHECK();
   cudaGraph_t body = add_while(c.stream, h);
   capture_body(c, body, 0, B_OUTER, [&] {
@@ -427,8 +474,8 @@ static void emit_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
 
 static int64_t graph_key(const SolveCfg& cfg, const Ctx& c) {
   return (int64_t)cfg.precision | ((int64_t)cfg.inner_pc << 2) | ((int64_t)cfg.use_guess << 3) |
-         ((int64_t)cfg.remove_rotation << 4) | ((int64_t)c.mg_degree << 5) | ((int64_t)c.mg.size() << 9) |
-         ((int64_t)(cfg.inner_relax > 0.0) << 14) | ((int64_t)c.mg_prec << 15) | ((int64_t)cfg.schur_pc << 17);
+         ((int64_t)cfg.remove_rotation << 5) | ((int64_t)c.mg_degree << 6) | ((int64_t)c.mg.size() << 10) |
+         ((int64_t)(cfg.inner_relax > 0.0) << 15) | ((int64_t)c.mg_prec << 16) | ((int64_t)cfg.schur_pc << 18);
 }
 
 void graph_free(Ctx& c) {
@@ -492,6 +539,8 @@ int schur_pcg_graph(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResu
   res.launches = c.gk_main + c.gk_body[B_OUTER] * o.outer_it + c.gk_body[B_PCG64] * o.in_total +
                  c.gk_body[B_PCG32] * o.in32_total + c.gk_body[B_REF] * o.ref_total;
   res.refinements = o.ref_total;
+  res.fallback = (cfg.use_guess == 2) ? (o.guess_used ? 0 : 1) : 0;
+  res.r0_guess = o.r0guess;
   res.r0 = o.r0;
   res.relres = o.r0 > 0 ? std::sqrt(c.h_scal[S_RR]) / o.r0 : 0.0;
   res.mom_residual = std::sqrt(c.h_scal[S_TMP] / std::max(c.h_scal[S_TMP2], 1e-300));

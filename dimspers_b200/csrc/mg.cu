@@ -177,7 +177,7 @@ __global__ void k_galerkin(const T* __restrict__ Kf, T* __restrict__ Kc, int nel
         if (pjl == 0.0) continue;
         const int r = 2 * i + alpha, cc = 2 * j + beta;
         const int pi = r >= cc ? packed_index12(r, cc) : packed_index12(cc, r);
-        s += pjl * (double)Kf[(size_t)pi * nelf + ef];
+        s += pjl * (double)Kf[kidx<T>(pi, ef)];
       }
       acc += pik * s;
     }
@@ -190,7 +190,7 @@ __global__ void k_galerkin(const T* __restrict__ Kf, T* __restrict__ Kc, int nel
   if (bl >= Bc) bl -= Bc;
   const int amax = 2 * ncrc;
   if (dof_fixed(ak, bk, alpha, amax, pin) || dof_fixed(al, bl, beta, amax, pin)) acc = 0.0;
-  Kc[(size_t)pidx * nelc + E] = (T)acc;
+  Kc[kidx<T>(pidx, E)] = (T)acc;
 }
 
 // ---- nodal 2x2 diagonal blocks and their inverses ----------------------------
@@ -202,9 +202,9 @@ __global__ void k_diag_blocks(const T* __restrict__ K, double* __restrict__ diag
   element_nodes_mg(e, ncr, A, B, nd);
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
-    atomicAdd(&diag[3 * nd[k] + 0], (double)K[(size_t)packed_index12(2 * k, 2 * k) * nel + e]);
-    atomicAdd(&diag[3 * nd[k] + 1], (double)K[(size_t)packed_index12(2 * k + 1, 2 * k) * nel + e]);
-    atomicAdd(&diag[3 * nd[k] + 2], (double)K[(size_t)packed_index12(2 * k + 1, 2 * k + 1) * nel + e]);
+    atomicAdd(&diag[3 * nd[k] + 0], (double)K[kidx<T>(packed_index12(2 * k, 2 * k), e)]);
+    atomicAdd(&diag[3 * nd[k] + 1], (double)K[kidx<T>(packed_index12(2 * k + 1, 2 * k), e)]);
+    atomicAdd(&diag[3 * nd[k] + 2], (double)K[kidx<T>(packed_index12(2 * k + 1, 2 * k + 1), e)]);
   }
 }
 
@@ -399,7 +399,7 @@ __global__ void k_dense_assemble(const T* __restrict__ K, double* __restrict__ D
   element_nodes_mg(e, ncr, A, B, nd);
   for (int C = 0; C < 12; ++C)
     for (int R = C; R < 12; ++R) {
-      const double v = (double)K[(size_t)packed_index12(R, C) * nel + e];
+      const double v = (double)K[kidx<T>(packed_index12(R, C), e)];
       const int gr = 2 * nd[R >> 1] + (R & 1), gc = 2 * nd[C >> 1] + (C & 1);
       atomicAdd(&D[(size_t)gr * n + gc], v);
       if (R != C) atomicAdd(&D[(size_t)gc * n + gr], v);
@@ -651,7 +651,7 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
     for (size_t l = 0; l < c.mg.size(); ++l) {
       MGLevel& L = c.mg[l];
       if (l > 0) {
-        DP_CUDA(cudaMalloc(prec ? (void**)&L.K32 : (void**)&L.K64, sizeof(T) * kKe * L.g.nel));
+        DP_CUDA(cudaMalloc(prec ? (void**)&L.K32 : (void**)&L.K64, sizeof(T) * kstore<T>(L.g.nel)));
       }
       DP_CUDA(cudaMalloc(prec ? (void**)&L.dinv32 : (void**)&L.dinv64, sizeof(T) * 3 * L.g.nnod));
       DP_CUDA(cudaMalloc(&L.cheb, sizeof(double) * 2 * (kMaxCheb + 1)));

@@ -15,11 +15,42 @@
 namespace dp {
 
 // ---- element-by-element K apply -------------------------------------------
+// Loads the element's packed matrix as 16-byte vectors (all issued before the
+// arithmetic, so each thread keeps 20-39 loads in flight), gathers x as one
+// 8/16-byte load per node and scatter-adds y per node (float2 vector atomics
+// for FP32).
+template <typename Tm>
+struct KVec;
+template <>
+struct KVec<float> { typedef float4 V; static constexpr int n = 20; };
+template <>
+struct KVec<double> { typedef double2 V; static constexpr int n = 39; };
+
+__device__ inline void vec_to(const float4& v, float* k) { k[0] = v.x; k[1] = v.y; k[2] = v.z; k[3] = v.w; }
+__device__ inline void vec_to(const double2& v, double* k) { k[0] = v.x; k[1] = v.y; }
+
+__device__ inline void atomic_add2(float* y, float a, float b) { atomicAdd(reinterpret_cast<float2*>(y), make_float2(a, b)); }
+__device__ inline void atomic_add2(double* y, double a, double b) { atomicAdd(y, a); atomicAdd(y + 1, b); }
+
+template <typename Tv>
+struct V2;
+template <>
+struct V2<float> { typedef float2 T; };
+template <>
+struct V2<double> { typedef double2 T; };
+
 template <typename Tm, typename Tv>
 __global__ void __launch_bounds__(128) k_apply_K(const Tm* __restrict__ K, const Tv* __restrict__ x,
                                                  Tv* __restrict__ y, int nel, int ncr, int A, int B) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nel) return;
+  typedef typename KVec<Tm>::V VT;
+  constexpr int NV = KVec<Tm>::n;
+  constexpr int PER = sizeof(VT) / sizeof(Tm);
+  const VT* Kb = reinterpret_cast<const VT*>(K + (int64_t)(e >> 5) * (32 * NV * PER)) + (e & 31);
+  Tm kk[NV * PER];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) vec_to(Kb[j * 32], kk + j * PER);
   const int q = e >> 1, t = e & 1;
   const int ir = q % ncr, it = q / ncr;
   const int a0 = 2 * ir, b0 = 2 * it;
@@ -36,11 +67,14 @@ __global__ void __launch_bounds__(128) k_apply_K(const Tm* __restrict__ K, const
 #pragma unroll
     for (int k = 0; k < 6; ++k) nd[k] = aa[k] + A * (bb[k] >= B ? bb[k] - B : bb[k]);
   }
+  typedef typename V2<Tv>::T X2;
+  const X2* x2 = reinterpret_cast<const X2*>(x);
   Tv xe[12], ye[12];
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
-    xe[2 * k] = x[2 * nd[k]];
-    xe[2 * k + 1] = x[2 * nd[k] + 1];
+    const X2 v = x2[nd[k]];
+    xe[2 * k] = v.x;
+    xe[2 * k + 1] = v.y;
     ye[2 * k] = 0;
     ye[2 * k + 1] = 0;
   }
@@ -48,16 +82,13 @@ __global__ void __launch_bounds__(128) k_apply_K(const Tm* __restrict__ K, const
   for (int C = 0; C < 12; ++C) {
 #pragma unroll
     for (int R = C; R < 12; ++R) {
-      const Tv kv = (Tv)K[(size_t)packed_index12(R, C) * nel + e];
+      const Tv kv = (Tv)kk[packed_index12(R, C)];
       ye[R] += kv * xe[C];
       if (R != C) ye[C] += kv * xe[R];
     }
   }
 #pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    atomicAdd(&y[2 * nd[k]], ye[2 * k]);
-    atomicAdd(&y[2 * nd[k] + 1], ye[2 * k + 1]);
-  }
+  for (int k = 0; k < 6; ++k) atomic_add2(&y[2 * nd[k]], ye[2 * k], ye[2 * k + 1]);
 }
 
 template <typename Tm, typename Tv>

@@ -16,7 +16,7 @@ struct SolveCfg {
   int inner_itmax = 500;
   int max_refine = 6;
   int remove_rotation = 1;
-  int use_guess = 0;
+  int use_guess = 0;        // 0 zero guess; 1 warm start from P; 2 learned guess with fallback
   int verbose = 0;
   int host_loop = 0;        // 1: host-driven loops (debug); 0: one CUDA graph per solve
   double inner_relax = 0.0; // > 0: relaxed inner tolerance with this cap
@@ -35,6 +35,8 @@ struct SolveResult {
   int64_t inner_its = 0;
   int64_t launches = 0;       // kernels launched by the solve
   int64_t refinements = 0;    // FP64 refinement steps (FP32-refined path)
+  int fallback = 0;           // learned guess rejected
+  double r0_guess = 0.0;      // ||r(P0)|| of the guess
   double relres = 0.0, r0 = 0.0, omega = 0.0, div_residual = 0.0, mom_residual = 0.0;
 };
 

@@ -19,6 +19,10 @@ Workloads (all on r in [1.22, 2.22], free slip, rotation removed):
            = sum of 8 Fourier modes in (theta, r) with seeded phases
   fabric   contrast 1e6; director = major eigenvector of F F^T per element,
            F = I + 0.5 G, G a seeded smooth 2x2 field (8 modes per component)
+  plumes   training workload of the learned guess: conductive profile plus
+           1-16 Gaussian plumes (radius 0.05-0.2, amplitude +-0.3, random
+           centres), Ra log-uniform in [1e5, 1e7], contrast 1e5, delta and
+           director as `aniso`
 """
 from dataclasses import dataclass
 
@@ -79,6 +83,22 @@ def temperature(theta, r, seed, amp_noise=1e-3):
     return T
 
 
+def plume_temperature(theta, r, seed):
+    u = uniform(seed, 5, 1 + 5 * 16)
+    nplume = 1 + int(u[0] * 16)
+    T = np.log(r / R_OUT) / np.log(R_IN / R_OUT)
+    x, z = r * np.sin(theta), r * np.cos(theta)
+    for k in range(nplume):
+        a, b, c, d, e = u[1 + 5 * k: 6 + 5 * k]
+        th_c = 2 * np.pi * a
+        r_c = R_IN + 0.1 + 0.8 * b
+        rad = 0.05 + 0.15 * c
+        amp = 0.3 * (2 * d - 1)
+        xc, zc = r_c * np.sin(th_c), r_c * np.cos(th_c)
+        T = T + amp * np.exp(-((x - xc) ** 2 + (z - zc) ** 2) / (rad * rad))
+    return T
+
+
 def eta_from_T(T, e2n, contrast):
     Tip = N7 @ T[e2n[:6]]                       # (7, nel)
     return np.ascontiguousarray(np.exp(-np.log(contrast) * Tip).T)
@@ -127,14 +147,18 @@ def _tile7(v):
 
 def make_material(mesh, kind="iso", seed=1, Ra=1e5, contrast=None):
     """mesh: object with theta, r (nodal), e2n (6, nel) 0-based, th_el, r_el (3, nel)."""
-    T = temperature(mesh.theta, mesh.r, seed)
+    if kind == "plumes":
+        T = plume_temperature(mesh.theta, mesh.r, seed)
+        Ra = float(10.0 ** (5.0 + 2.0 * uniform(seed, 6, 1)[0]))
+    else:
+        T = temperature(mesh.theta, mesh.r, seed)
     nel = mesh.e2n.shape[1]
     if kind == "iso":
         eta = eta_from_T(T, mesh.e2n, contrast or 1e3)
         return Material(eta_ip=eta, rho=T.copy(), g=Ra, T=T)
     thc, rc = centroids(mesh.th_el, mesh.r_el)
     delta = 1.0 + 9.0 * uniform(seed, 2, nel)
-    if kind == "aniso":
+    if kind in ("aniso", "plumes"):
         eta = eta_from_T(T, mesh.e2n, contrast or 1e5)
         phi = fourier_field(thc, rc, seed, 3)
         dx, dy = np.cos(phi), np.sin(phi)

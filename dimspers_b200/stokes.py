@@ -224,7 +224,7 @@ class StokesContext:
         o = default_opts(**opts)
         U = np.zeros(2 * self.nnod)
         P = np.zeros(self.npres) if P0 is None else np.array(P0, dtype=np.float64)
-        if P0 is not None:
+        if P0 is not None and o.use_guess == 0:
             o.use_guess = 1
         Uc = np.zeros(2 * self.nnod) if want_cart else None
         rep = SolveReport()

@@ -69,7 +69,12 @@ typedef struct {
   double inner_rtol;       /* inner K-solve relative tolerance                */
   int32_t inner_itmax;     /* inner iteration cap                             */
   int32_t remove_rotation; /* apply updatevelocity2's rigid-rotation removal  */
-  int32_t use_guess;       /* 1: start from the P passed in (else P = 0)      */
+  int32_t use_guess;       /* 0: P = 0 (StokesPcCG); 1: warm start from the P
+                              passed in, tolerance relative to its own r0 (as
+                              StokesPcCG_pardiso keeps U, P); 2: learned guess:
+                              start from the P passed in only if its Schur
+                              residual is below the zero guess's, and stop at
+                              rtol relative to the zero-guess residual       */
   int32_t verbose;
   int32_t cheb_degree;     /* Chebyshev smoothing steps per level             */
   double inner_rtol32;     /* FP32 inner tolerance per refinement step        */
@@ -104,6 +109,8 @@ typedef struct {
   int32_t mg_levels;
   int64_t kernel_launches;     /* kernels this library launched for the solve */
   int64_t refinements;         /* FP64 refinement steps (FP32-refined path)   */
+  double r0_guess;             /* use_guess = 2: ||r(P0)|| of the guess; r0 is then
+                                  the zero-guess residual                     */
 } dp_solve_report;
 
 typedef struct dp_ctx dp_ctx;
@@ -195,6 +202,30 @@ void dp_default_opts(dp_solve_opts* opts);
  * device share that array: calls that overlap on the GPU race.  The first call
  * on a device looks up the array's address; make it before any stream capture. */
 int dp_apply_K_noalloc(dp_ctx* ctx, const double* x, double* y);
+
+/* ---- learned initial guess ----------------------------------------------
+ * A small convolutional network on the polar grid of the half-resolution
+ * mesh's vertices (nrg = ncr/2 + 1 radial x ntg = nct/2 angular, periodic in
+ * theta) predicts P/g; dp_guess_from_grid prolongates it to the pressure DOFs
+ * for dp_solve with use_guess = 2.  Forward, backward and Adam run in this
+ * library's own kernels.  Activations: [batch][channel][r][theta], FP32,
+ * device pointers.  (No counterpart in the reference, whose StokesPcCG starts
+ * from P = 0.) */
+typedef struct dp_cnn dp_cnn;
+int dp_cnn_create(int32_t nrg, int32_t ntg, int32_t channels, int32_t layers, const int32_t* dilations,
+                  int32_t max_batch, int32_t device, dp_cnn** out);
+void dp_cnn_destroy(dp_cnn* net);
+int64_t dp_cnn_num_params(const dp_cnn* net);
+int dp_cnn_set_params(dp_cnn* net, const float* params, int64_t n);          /* host; resets Adam */
+int dp_cnn_get_params(dp_cnn* net, float* params, float* grads, int64_t n);   /* host; either may be NULL */
+int dp_cnn_forward(dp_cnn* net, const float* x, float* y, int32_t batch);
+int dp_cnn_gradients(dp_cnn* net, const float* x, const float* target, int32_t batch, double* loss);
+int dp_cnn_train_step(dp_cnn* net, const float* x, const float* target, int32_t batch, float lr, double* loss);
+/* Network inputs (rho, log10 eta, cos 2phi, sin 2phi) of the context's material on its grid. */
+int dp_cnn_inputs(dp_ctx* ctx, float* x, int32_t nrg, int32_t ntg);
+/* P = scale * (grid field, bilinear at the element vertices) -> pressure DOFs. */
+int dp_guess_from_grid(dp_ctx* ctx, const float* p_grid, int32_t nrg, int32_t ntg, double scale, double* P,
+                       int32_t mem);
 
 /* Average device time (ms) of one launch of a hot kernel on the context's
  * stream, from CUDA events, after an assembly: which = 0 fine-level A-apply

@@ -1,0 +1,118 @@
+"""The learned-guess network's hand-written CUDA kernels against a torch-CPU
+reference of the same network (forward, loss and every parameter gradient),
+a training smoke test, and the solver's guess selection / fallback."""
+import numpy as np
+import pytest
+
+from conftest import rel
+from dimspers_b200 import StokesContext, build_mesh, inputs, learned
+
+pytestmark = pytest.mark.gpu
+
+
+def torch_reference(params, x, t, nrg, ntg, channels, layers, dil):
+    import torch
+    import torch.nn.functional as F
+    p = torch.tensor(params, dtype=torch.float64, requires_grad=True)
+    h = torch.tensor(x, dtype=torch.float64)
+    off = 0
+    for l in range(layers):
+        cin = 4 if l == 0 else channels
+        cout = 1 if l == layers - 1 else channels
+        W = p[off:off + cout * cin * 9].view(cout, cin, 3, 3)
+        off += cout * cin * 9
+        b = p[off:off + cout]
+        off += cout
+        d = dil[l]
+        hp = F.pad(h, (d, d, 0, 0), mode="circular")        # periodic in theta (last dim)
+        hp = F.pad(hp, (0, 0, d, d))                        # zero in r
+        h = F.conv2d(hp, W, b, dilation=d)
+        if l < layers - 1:
+            h = torch.relu(h)
+    loss = ((h - torch.tensor(t, dtype=torch.float64)) ** 2).mean()
+    loss.backward()
+    return h.detach().numpy(), float(loss), p.grad.numpy()
+
+
+def test_network_gradients_match_torch_cpu():
+    import torch
+    nrg, ntg, C, L, dil = 6, 16, 8, 4, (1, 2, 3, 1)
+    net = learned.GuessNet(nrg, ntg, C, L, dil, max_batch=2)
+    net.init_params(seed=3)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((2, 4, nrg, ntg)).astype(np.float32)
+    t = rng.standard_normal((2, 1, nrg, ntg)).astype(np.float32)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    yd = torch.empty((2, 1, nrg, ntg), dtype=torch.float32, device="cuda")
+    net.forward(xd, yd)
+    loss = net.gradients(xd, td)
+    params, grads = net.get_params(grads=True)
+    y_ref, loss_ref, g_ref = torch_reference(params, x, t, nrg, ntg, C, L, dil)
+    assert rel(yd.cpu().numpy(), y_ref) < 1e-5
+    assert abs(loss - loss_ref) < 1e-5 * abs(loss_ref)
+    assert rel(grads, g_ref) < 1e-4
+    net.close()
+
+
+def test_network_trains():
+    import torch
+    nrg, ntg = 9, 32
+    net = learned.GuessNet(nrg, ntg, 8, 4, (1, 2, 1, 1), max_batch=4)
+    net.init_params(seed=1)
+    rng = np.random.default_rng(1)
+    x = torch.from_numpy(rng.standard_normal((4, 4, nrg, ntg)).astype(np.float32)).cuda()
+    t = (0.5 * x[:, :1] - 0.25 * x[:, 1:2]).contiguous()
+    first = net.train_step(x, t, 1e-2)
+    for _ in range(300):
+        last = net.train_step(x, t, 3e-3)
+    assert last < 0.2 * first
+    net.close()
+
+
+def test_solver_keeps_a_good_guess_and_rejects_a_bad_one():
+    mesh = build_mesh(8, 64, "discontinuous")
+    mat = inputs.make_material(mesh, "aniso", seed=5)
+    with StokesContext(8, 64, "discontinuous") as ctx:
+        ctx.set_material(mat.eta_ip, mat.rho, mat.g, mat.C6)
+        ctx.assemble(1)
+        opts = dict(precision=1, rtol=1e-8, itmax=5000)
+        U0, P0, _, r0 = ctx.solve(**opts)
+        Ptight = ctx.solve(precision=1, rtol=1e-11, itmax=5000)[1]
+        # near-exact guess: kept, far fewer iterations, same answer
+        _, P1, _, r1 = ctx.solve(P0=Ptight * (1 + 1e-3), use_guess=2, **opts)
+        assert r1["fallback_used"] == 0 and r1["iterations"] < r0["iterations"] // 2
+        assert abs(r1["r0"] - r0["r0"]) < 1e-9 * r0["r0"]           # tolerance from the zero guess
+        assert rel(P1, P0) < 1e-4
+        # garbage guess: rejected, identical to the zero-guess solve
+        bad = np.random.default_rng(0).standard_normal(ctx.npres) * 1e3 * np.abs(Ptight).max()
+        _, P2, _, r2 = ctx.solve(P0=bad, use_guess=2, **opts)
+        assert r2["fallback_used"] == 1 and r2["r0_guess"] > r2["r0"]
+        assert r2["iterations"] == r0["iterations"]
+        assert rel(P2, P0) < 1e-6   # same iterations; atomics reorder FP64 sums
+
+
+def test_guess_pipeline_shapes():
+    """features -> network -> prolongation produce finite pressure DOFs."""
+    import torch
+    mesh = build_mesh(8, 64, "discontinuous")
+    mat = inputs.make_material(mesh, "plumes", seed=9)
+    nrg, ntg = learned.grid_shape(8, 64)
+    net = learned.GuessNet(nrg, ntg, 8, 3, (1, 2, 1), max_batch=1)
+    net.init_params(seed=0)
+    with StokesContext(8, 64, "discontinuous") as ctx:
+        ctx.set_material_ti(mat.eta_ip, mat.rho, mat.g, mat.delta, mat.dir_x, mat.dir_y)
+        X = torch.empty((1, 4, nrg, ntg), dtype=torch.float32, device="cuda")
+        learned.features(ctx, X)
+        Xh = X.cpu().numpy()
+        assert np.allclose(Xh[0, 0], mat.rho[np.array([[mesh_vertex(ctx, 2 * i, 2 * j) for j in range(ntg)]
+                                                       for i in range(nrg)])], atol=1e-6)
+        g = learned.LearnedGuess(net, ctx)
+        P0 = np.zeros(ctx.npres)
+        g.predict(mat.g, P0.ctypes.data, mem=0)
+        assert np.all(np.isfinite(P0)) and np.abs(P0).max() > 0
+    net.close()
+
+
+def mesh_vertex(ctx, ir, it):
+    """reference node number of the vertex (ir, it): ir + (ncr + 1) * it"""
+    return ir + (ctx.desc.nr_cells + 1) * it
