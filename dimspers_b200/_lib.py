@@ -30,7 +30,8 @@ class SolveOpts(C.Structure):
                 ("verbose", C.c_int32), ("cheb_degree", C.c_int32), ("inner_rtol32", C.c_double),
                 ("max_refine", C.c_int32), ("host_loop", C.c_int32), ("block_jacobi", C.c_int32),
                 ("cheb_lo", C.c_double), ("cheb_hi", C.c_double), ("inner_relax", C.c_double),
-                ("coarse_max", C.c_int32), ("schur_pc", C.c_int32)]
+                ("coarse_max", C.c_int32), ("schur_pc", C.c_int32),
+                ("apply_warps", C.c_int32), ("apply_warps_t", C.c_int32)]
 
 
 class SolveReport(C.Structure):
@@ -74,6 +75,10 @@ SIGNATURES = {
     "dp_get_rhs": (C.c_int, [_P, _P, _P]),
     "dp_default_opts": (None, [C.POINTER(SolveOpts)]),
     "dp_profile_kernel": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
+    "dp_batch_create": (C.c_int, [C.POINTER(_P), C.c_int32, _P, C.POINTER(_P)]),
+    "dp_batch_run": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.c_int32, _P,
+                               C.POINTER(C.c_double)]),
+    "dp_batch_destroy": (None, [_P]),
     "dp_cnn_create": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, _I32, C.c_int32, C.c_int32,
                                 C.POINTER(_P)]),
     "dp_cnn_destroy": (None, [_P]),

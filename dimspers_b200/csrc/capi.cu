@@ -122,6 +122,13 @@ static SolveCfg make_cfg(const dp_solve_opts* o) {
   if (o->coarse_max > 0) cfg.mg.coarse_max = o->coarse_max;
   cfg.schur_pc = o->schur_pc;
   if (cfg.schur_pc != 0 && cfg.schur_pc != 1) throw BadArg("schur_pc must be 0 (lumped) or 1 (mass)");
+  if (o->apply_warps > 0) cfg.mg.apply_warps = o->apply_warps;
+  if (o->apply_warps_t > 0) cfg.mg.apply_warps_t = o->apply_warps_t;
+  {
+    const int w = cfg.mg.apply_warps, wt = cfg.mg.apply_warps_t;
+    if (w != 1 && w != 2 && w != 4 && w != 8) throw BadArg("apply_warps must be 1, 2, 4 or 8");
+    if ((wt & (wt - 1)) != 0 || wt > w) throw BadArg("apply_warps_t must be a power of two <= apply_warps");
+  }
   if (cfg.inner_pc != 0 && cfg.inner_pc != 1) throw BadArg("inner_pc must be 0 or 1");
   return cfg;
 }
@@ -135,11 +142,157 @@ __global__ void k_f64_to_f32(const double* a, float* b, int64_t nel) {
   b[kidx32(p, e)] = (float)a[kidx64(p, e)];
 }
 
+// FP32 copy of the operator when a mode needs it, then the multigrid values
+// (Galerkin operators, smoother bounds, coarse inverse) for the current assembly.
+static void check_solve_cfg(const Ctx& c, const SolveCfg& cfg) {
+  if (c.assembled < 0) throw BadArg("dp_assemble must run before solving");
+  if (cfg.schur_pc == 1 && c.mesh.pressure != 1)
+    throw BadArg("schur_pc = 1 (element-block mass inverse) needs discontinuous pressure");
+  if (cfg.use_guess < 0 || cfg.use_guess > 2) throw BadArg("use_guess must be 0, 1 or 2");
+  if (cfg.use_guess == 2 && cfg.host_loop) throw BadArg("the learned-guess mode runs in the graph path only");
+}
+
+// FP32 copy of the assembled operator (once per assembly) for the FP32 modes.
+static void ensure_k32(Ctx& c, const SolveCfg& cfg) {
+  if (cfg.precision >= 1 && c.assembled == 0) {
+    if (!c.K32) {
+      dalloc(&c.K32, kstore<float>(c.fine.nel));
+      DP_CUDA(cudaMemsetAsync(c.K32, 0, sizeof(float) * kstore<float>(c.fine.nel), c.stream));
+    }
+    const int64_t n = kKe * c.fine.nel;
+    ++g_klaunch;
+    k_f64_to_f32<<<(int)div_up(n, 256), 256, 0, c.stream>>>(c.K64, c.K32, c.fine.nel);
+    DP_LAUNCH_CHECK();
+    c.assembled = 1;
+  }
+}
+
+// Checks, the FP32 operator when needed, then the multigrid values (Galerkin
+// operators, smoother bounds, coarse inverse) of the current assembly.
+static void prepare_solve(Ctx& c, const SolveCfg& cfg) {
+  check_solve_cfg(c, cfg);
+  c.fine.warps = cfg.mg.apply_warps;
+  c.fine.warps_t = cfg.mg.apply_warps_t;
+  ensure_k32(c, cfg);
+  mg_setup(c, cfg.precision >= 1 ? 1 : 0, cfg.mg);
+}
+
+// Solution (lattice, work vectors) -> caller's arrays in the reference numbering.
+static void deliver_solution(Ctx& c, double* U, double* P, double* Ucart, int mem) {
+  const int64_t nn = c.fine.nnod, np = c.mesh.npres;
+  double* dU = (double*)c.work[W_U];
+  double* dP = (double*)c.work[W_P];
+  double* stage = (double*)c.work[W_UC];
+  if (U) {
+    launch_scatter_lat2ref(c, dU, stage, 2);
+    DP_CUDA(cudaMemcpyAsync(U, stage, sizeof(double) * 2 * nn, kind_out(mem), c.stream));
+  }
+  if (P) DP_CUDA(cudaMemcpyAsync(P, dP, sizeof(double) * np, kind_out(mem), c.stream));
+  if (Ucart) {
+    double* uc = (double*)c.work[W_RES];
+    to_cartesian(c, dU, uc);
+    launch_scatter_lat2ref(c, uc, stage, 2);
+    DP_CUDA(cudaMemcpyAsync(Ucart, stage, sizeof(double) * 2 * nn, kind_out(mem), c.stream));
+  }
+}
+
+static void fill_report(const Ctx& c, const SolveResult& res, dp_solve_report* rep) {
+  if (!rep) return;
+  std::memset(rep, 0, sizeof(*rep));
+  rep->status = res.status;
+  rep->iterations = res.iterations;
+  rep->inner_iterations = res.inner_its;
+  rep->relres = res.relres;
+  rep->r0 = res.r0;
+  rep->omega = res.omega;
+  rep->div_residual = res.div_residual;
+  rep->mom_residual = res.mom_residual;
+  rep->mg_levels = (int)c.mg.size();
+  rep->kernel_launches = res.launches;
+  rep->refinements = res.refinements;
+  rep->fallback_used = res.fallback;
+  rep->r0_guess = res.r0_guess;
+}
+
 }  // namespace dp
+
+struct dp_batch {
+  dp::Batch b;
+};
 
 using namespace dp;
 
 extern "C" {
+
+int dp_batch_create(dp_ctx* const* ctxs, int32_t n, const dp_solve_opts* opts, dp_batch** out) {
+  if (!ctxs || n < 1 || !out) return DP_BAD_ARG;
+  *out = nullptr;
+  dp_batch* h = nullptr;
+  int st = guarded(nullptr, [&] {
+    h = new dp_batch();
+    const int dev = ctxs[0] ? ctxs[0]->c.device : 0;
+    DP_CUDA(cudaSetDevice(dev));
+    for (int i = 0; i < n; ++i) {
+      if (!ctxs[i]) throw BadArg("null context in batch");
+      Ctx& c = ctxs[i]->c;
+      if (c.device != dev) throw BadArg("all contexts of a batch must be on one device");
+      for (int j = 0; j < i; ++j)
+        if (ctxs[j] == ctxs[i]) throw BadArg("a context appears twice in the batch");
+      SolveCfg cfg = make_cfg(opts ? &opts[i] : nullptr);
+      if (cfg.host_loop) throw BadArg("batches run in the graph path only");
+      prepare_solve(c, cfg);
+      DP_CUDA(cudaStreamSynchronize(c.stream));
+      h->b.ctx.push_back(&c);
+      h->b.cfg.push_back(cfg);
+    }
+    batch_build(h->b);
+    return (int)DP_OK;
+  });
+  if (st != DP_OK) {
+    delete h;
+    return st;
+  }
+  *out = h;
+  return DP_OK;
+}
+
+int dp_batch_run(dp_batch* h, double* const* P_guess, double* const* U, double* const* P, int32_t mem,
+                 dp_solve_report* reports, double* done_ms) {
+  if (!h) return DP_BAD_ARG;
+  Batch& b = h->b;
+  int st = guarded(nullptr, [&] {
+    const int n = (int)b.ctx.size();
+    DP_CUDA(cudaSetDevice(b.ctx[0]->device));
+    for (int i = 0; i < n; ++i) {
+      Ctx& c = *b.ctx[i];
+      prepare_solve(c, b.cfg[i]);   // multigrid values of the current assembly
+      if (b.cfg[i].use_guess) {
+        if (!P_guess || !P_guess[i]) throw BadArg("use_guess needs a guess for every problem");
+        DP_CUDA(cudaMemcpyAsync(c.work[W_P], P_guess[i], sizeof(double) * c.mesh.npres, kind_in(mem), c.stream));
+      }
+      DP_CUDA(cudaStreamSynchronize(c.stream));
+    }
+    std::vector<SolveResult> res;
+    std::vector<double> ms;
+    batch_run(b, res, ms);
+    for (int i = 0; i < n; ++i) {
+      Ctx& c = *b.ctx[i];
+      deliver_solution(c, U ? U[i] : nullptr, P ? P[i] : nullptr, nullptr, mem);
+      DP_CUDA(cudaStreamSynchronize(c.stream));
+      fill_report(c, res[i], reports ? &reports[i] : nullptr);
+      if (done_ms) done_ms[i] = ms[i];
+    }
+    return (int)DP_OK;
+  });
+  if (st != DP_OK) b.err = g_err;
+  return st;
+}
+
+void dp_batch_destroy(dp_batch* h) {
+  if (!h) return;
+  if (h->b.s) cudaStreamSynchronize(h->b.s);
+  delete h;
+}
 
 void dp_default_opts(dp_solve_opts* o) {
   if (!o) return;
@@ -163,6 +316,8 @@ void dp_default_opts(dp_solve_opts* o) {
   o->cheb_hi = 1.1;
   o->inner_relax = 0.0;
   o->coarse_max = 1024;
+  o->apply_warps = 4;
+  o->apply_warps_t = 1;
 }
 
 const char* dp_status_string(int s) {
@@ -433,22 +588,12 @@ int dp_solve(dp_ctx* h, double* U, double* P, double* Ucart, const dp_solve_opts
   return guarded(&c, [&] {
     DP_CUDA(cudaSetDevice(c.device));
     if (!U || !P) throw BadArg("null U or P");
-    if (c.assembled < 0) throw BadArg("dp_assemble must run before dp_solve");
     SolveCfg cfg = make_cfg(opts);
-    if (cfg.schur_pc == 1 && c.mesh.pressure != 1)
-      throw BadArg("schur_pc = 1 (element-block mass inverse) needs discontinuous pressure");
+    check_solve_cfg(c, cfg);
+    c.fine.warps = cfg.mg.apply_warps;
+    c.fine.warps_t = cfg.mg.apply_warps_t;
     const int64_t nn = c.fine.nnod, np = c.mesh.npres;
-    if (cfg.precision >= 1 && c.assembled == 0) {
-      if (!c.K32) {
-        dalloc(&c.K32, kstore<float>(c.fine.nel));
-        DP_CUDA(cudaMemsetAsync(c.K32, 0, sizeof(float) * kstore<float>(c.fine.nel), c.stream));
-      }
-      const int64_t n = kKe * c.fine.nel;
-      ++g_klaunch;
-      k_f64_to_f32<<<(int)div_up(n, 256), 256, 0, c.stream>>>(c.K64, c.K32, c.fine.nel);
-      DP_LAUNCH_CHECK();
-      c.assembled = 1;
-    }
+    ensure_k32(c, cfg);
     cudaEvent_t e0, e1, e2;
     DP_CUDA(cudaEventCreate(&e0));
     DP_CUDA(cudaEventCreate(&e1));
@@ -458,8 +603,6 @@ int dp_solve(dp_ctx* h, double* U, double* P, double* Ucart, const dp_solve_opts
     DP_CUDA(cudaEventRecord(e1, c.stream));
     double* dU = (double*)c.work[W_U];
     double* dP = (double*)c.work[W_P];
-    if (cfg.use_guess < 0 || cfg.use_guess > 2) throw BadArg("use_guess must be 0, 1 or 2");
-    if (cfg.use_guess == 2 && cfg.host_loop) throw BadArg("the learned-guess mode runs in the graph path only");
     if (cfg.use_guess) {
       DP_CUDA(cudaMemcpyAsync(dP, P, sizeof(double) * np, kind_in(mem), c.stream));
     }
@@ -473,39 +616,17 @@ int dp_solve(dp_ctx* h, double* U, double* P, double* Ucart, const dp_solve_opts
       schur_pcg_graph(c, cfg, dU, dP, res);
     }
     // lattice -> reference numbering
-    double* stage = (double*)c.work[W_UC];
-    launch_scatter_lat2ref(c, dU, stage, 2);
-    DP_CUDA(cudaMemcpyAsync(U, stage, sizeof(double) * 2 * nn, kind_out(mem), c.stream));
-    DP_CUDA(cudaMemcpyAsync(P, dP, sizeof(double) * np, kind_out(mem), c.stream));
-    if (Ucart) {
-      double* uc = (double*)c.work[W_RES];
-      to_cartesian(c, dU, uc);
-      launch_scatter_lat2ref(c, uc, stage, 2);
-      DP_CUDA(cudaMemcpyAsync(Ucart, stage, sizeof(double) * 2 * nn, kind_out(mem), c.stream));
-    }
+    deliver_solution(c, U, P, Ucart, mem);
     DP_CUDA(cudaEventRecord(e2, c.stream));
     DP_CUDA(cudaStreamSynchronize(c.stream));
     float ms_setup = 0, ms_solve = 0;
     cudaEventElapsedTime(&ms_setup, e0, e1);
     cudaEventElapsedTime(&ms_solve, e1, e2);
     cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
+    fill_report(c, res, rep);
     if (rep) {
-      std::memset(rep, 0, sizeof(*rep));
-      rep->status = res.status;
-      rep->iterations = res.iterations;
-      rep->inner_iterations = res.inner_its;
-      rep->relres = res.relres;
-      rep->r0 = res.r0;
-      rep->omega = res.omega;
-      rep->div_residual = res.div_residual;
-      rep->mom_residual = res.mom_residual;
       rep->t_setup_ms = ms_setup;
       rep->t_solve_ms = ms_solve;
-      rep->mg_levels = (int)c.mg.size();
-      rep->kernel_launches = res.launches;
-      rep->refinements = res.refinements;
-      rep->fallback_used = res.fallback;
-      rep->r0_guess = res.r0_guess;
     }
     if (res.status == 1) c.err = "outer iteration cap reached";
     if (res.status == 2) c.err = "breakdown: q.Sq <= 0 or non-finite scalar";

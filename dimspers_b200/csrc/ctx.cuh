@@ -39,6 +39,10 @@ struct Level {
   int ncr = 0, nct = 0;
   int pin = 0;               // u_theta of lattice node (2*ncr, 0) is fixed
   int64_t nel = 0, nnod = 0;
+  // Tile of the element-by-element applies: a CTA of `warps` warps, `warps_t` of
+  // them stacked along theta (each warp = 16 radial cells x 2 triangles); the
+  // stacked form needs ncr % 16 == 0 and falls back to the linear element order.
+  int warps = 4, warps_t = 1;
   int64_t A() const { return 2 * (int64_t)ncr + 1; }
   int64_t B() const { return 2 * (int64_t)nct; }
 };
@@ -101,6 +105,7 @@ struct Ctx {
   int mg_prec = -1;             // 0 = fp64, 1 = fp32
   int mg_degree = 3;            // Chebyshev steps in use
   int64_t mg_coarse_max = -1;   // coarse_max the hierarchy was built for
+  int64_t alloc_gen = 0;        // bumped whenever buffers a captured graph may hold are freed
   double* coarse_chol = nullptr;// dense Cholesky factor of the coarsest level
   int64_t coarse_n = 0;
   int64_t* coarse_map = nullptr;// coarsest DOF -> dense index (-1 fixed)
@@ -119,6 +124,7 @@ struct Ctx {
   void* graph = nullptr;        // cudaGraph_t
   void* gexec = nullptr;        // cudaGraphExec_t
   int64_t gkey = -1;
+  int64_t ggen = -1;            // alloc_gen the cached graph was captured with
   const void* gU = nullptr;
   const void* gP = nullptr;
   int64_t gk_main = 0;          // kernel nodes outside loop bodies

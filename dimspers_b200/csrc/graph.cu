@@ -475,7 +475,9 @@ static void emit_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
 static int64_t graph_key(const SolveCfg& cfg, const Ctx& c) {
   return (int64_t)cfg.precision | ((int64_t)cfg.inner_pc << 2) | ((int64_t)cfg.use_guess << 3) |
          ((int64_t)cfg.remove_rotation << 5) | ((int64_t)c.mg_degree << 6) | ((int64_t)c.mg.size() << 10) |
-         ((int64_t)(cfg.inner_relax > 0.0) << 15) | ((int64_t)c.mg_prec << 16) | ((int64_t)cfg.schur_pc << 18);
+         ((int64_t)(cfg.inner_relax > 0.0) << 15) | ((int64_t)c.mg_prec << 16) | ((int64_t)cfg.schur_pc << 18) |
+         ((int64_t)cfg.mg.block_jacobi << 20) | ((int64_t)(c.coarse_n > 0) << 21) |
+         ((int64_t)cfg.mg.apply_warps << 24) | ((int64_t)cfg.mg.apply_warps_t << 28);
 }
 
 void graph_free(Ctx& c) {
@@ -486,37 +488,24 @@ void graph_free(Ctx& c) {
   c.gkey = -1;
 }
 
-int schur_pcg_graph(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& res) {
+static void ensure_ctl(Ctx& c) {
   if (!c.ctl) {
     DP_CUDA(cudaMalloc(&c.ctl, sizeof(DevCtl)));
     DP_CUDA(cudaMallocHost(&c.h_ctl, sizeof(DevCtl)));
     for (int i = 0; i < 3; ++i) DP_CUDA(cudaStreamCreateWithFlags(&c.aux[i], cudaStreamNonBlocking));
   }
-  const int64_t key = graph_key(cfg, c);
-  if (!c.gexec || c.gkey != key || c.gU != U || c.gP != P) {
-    graph_free(c);
-    DP_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed));
-    const int64_t start = g_klaunch;
-    c.cap_nested = 0;
-    try {
-      emit_solve(c, cfg, U, P);
-    } catch (...) {
-      cudaGraph_t g = nullptr;
-      cudaStreamEndCapture(c.stream, &g);
-      if (g) cudaGraphDestroy(g);
-      throw;
-    }
-    cudaGraph_t g = nullptr;
-    DP_CUDA(cudaStreamEndCapture(c.stream, &g));
-    c.gk_main = (g_klaunch - start) - c.cap_nested;
-    cudaGraphExec_t ex = nullptr;
-    DP_CUDA(cudaGraphInstantiate(&ex, g, 0));
-    c.graph = g;
-    c.gexec = ex;
-    c.gkey = key;
-    c.gU = U;
-    c.gP = P;
-  }
+}
+
+// Captures the solve of c (on c.stream, which may be part of an enclosing
+// capture) and records its kernel-count bookkeeping.
+static void capture_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
+  const int64_t start = g_klaunch;
+  c.cap_nested = 0;
+  emit_solve(c, cfg, U, P);
+  c.gk_main = (g_klaunch - start) - c.cap_nested;
+}
+
+static void upload_params(Ctx& c, const SolveCfg& cfg, cudaStream_t s) {
   DevCtl h{};
   h.rtol = cfg.rtol;
   h.inner_rtol = cfg.inner_rtol;
@@ -527,26 +516,152 @@ int schur_pcg_graph(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResu
   h.inner_itmax = cfg.inner_itmax;
   h.max_refine = cfg.max_refine;
   *(DevCtl*)c.h_ctl = h;
-  DP_CUDA(cudaMemcpyAsync(c.ctl, c.h_ctl, sizeof(DevCtl), cudaMemcpyHostToDevice, c.stream));
-  DP_CUDA(cudaGraphLaunch((cudaGraphExec_t)c.gexec, c.stream));
-  DP_CUDA(cudaMemcpyAsync(c.h_ctl, c.ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, c.stream));
-  DP_CUDA(cudaMemcpyAsync(c.h_scal, c.scal, sizeof(double) * 32, cudaMemcpyDeviceToHost, c.stream));
-  DP_CUDA(cudaStreamSynchronize(c.stream));
+  DP_CUDA(cudaMemcpyAsync(c.ctl, c.h_ctl, sizeof(DevCtl), cudaMemcpyHostToDevice, s));
+}
+
+// Reads the device control block and scalars of a finished solve (synchronises s).
+static void collect_result(Ctx& c, const SolveCfg& cfg, cudaStream_t s, SolveResult& res) {
+  DP_CUDA(cudaMemcpyAsync(c.h_ctl, c.ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, s));
+  DP_CUDA(cudaMemcpyAsync(c.h_scal, c.scal, sizeof(double) * 32, cudaMemcpyDeviceToHost, s));
+  DP_CUDA(cudaStreamSynchronize(s));
   const DevCtl& o = *(const DevCtl*)c.h_ctl;
   res.status = o.status;
   res.iterations = o.outer_it;
+  res.r0 = o.r0;
+  res.relres = o.r0 > 0 ? std::sqrt(c.h_scal[S_RR]) / o.r0 : 0.0;
+  res.mom_residual = std::sqrt(c.h_scal[S_TMP] / std::max(c.h_scal[S_TMP2], 1e-300));
+  res.div_residual = o.r0 > 0 ? std::sqrt(c.h_scal[G_TMP3]) / o.r0 : 0.0;
+  res.omega = cfg.remove_rotation ? c.h_scal[S_AM] / c.h_scal[S_MOM] : 0.0;
   res.inner_its = cfg.precision == 2 ? o.in32_total : o.in_total;
   res.launches = c.gk_main + c.gk_body[B_OUTER] * o.outer_it + c.gk_body[B_PCG64] * o.in_total +
                  c.gk_body[B_PCG32] * o.in32_total + c.gk_body[B_REF] * o.ref_total;
   res.refinements = o.ref_total;
   res.fallback = (cfg.use_guess == 2) ? (o.guess_used ? 0 : 1) : 0;
   res.r0_guess = o.r0guess;
-  res.r0 = o.r0;
-  res.relres = o.r0 > 0 ? std::sqrt(c.h_scal[S_RR]) / o.r0 : 0.0;
-  res.mom_residual = std::sqrt(c.h_scal[S_TMP] / std::max(c.h_scal[S_TMP2], 1e-300));
-  res.div_residual = o.r0 > 0 ? std::sqrt(c.h_scal[G_TMP3]) / o.r0 : 0.0;
-  res.omega = cfg.remove_rotation ? c.h_scal[S_AM] / c.h_scal[S_MOM] : 0.0;
+}
+
+int schur_pcg_graph(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& res) {
+  ensure_ctl(c);
+  const int64_t key = graph_key(cfg, c);
+  if (!c.gexec || c.gkey != key || c.gU != U || c.gP != P || c.ggen != c.alloc_gen) {
+    graph_free(c);
+    DP_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed));
+    try {
+      capture_solve(c, cfg, U, P);
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(c.stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    cudaGraph_t g = nullptr;
+    DP_CUDA(cudaStreamEndCapture(c.stream, &g));
+    cudaGraphExec_t ex = nullptr;
+    DP_CUDA(cudaGraphInstantiate(&ex, g, 0));
+    c.graph = g;
+    c.gexec = ex;
+    c.gkey = key;
+    c.gU = U;
+    c.gP = P;
+    c.ggen = c.alloc_gen;
+  }
+  upload_params(c, cfg, c.stream);
+  DP_CUDA(cudaGraphLaunch((cudaGraphExec_t)c.gexec, c.stream));
+  collect_result(c, cfg, c.stream, res);
   return res.status;
+}
+
+// ---- batches: independent solves of several contexts in ONE graph launch ------------
+// The graph is captured with a fork/join over the contexts' streams: one branch per
+// context holds that context's whole solve (its own WHILE nodes and device control
+// block).  An external event-record node at the end of each branch timestamps its
+// completion; a second (capture-internal) event joins the branch back.
+struct Batch {
+  std::vector<Ctx*> ctx;
+  std::vector<SolveCfg> cfg;
+  std::vector<int64_t> gen;   // each context's allocation generation at capture
+  cudaStream_t s = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t fork = nullptr, start = nullptr;
+  std::vector<cudaEvent_t> done, join;
+  std::string err;
+  void free_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+  ~Batch() {
+    free_graph();
+    for (cudaEvent_t e : done) cudaEventDestroy(e);
+    for (cudaEvent_t e : join) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (start) cudaEventDestroy(start);
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
+void batch_build(Batch& b) {
+  if (!b.s) {
+    DP_CUDA(cudaStreamCreateWithFlags(&b.s, cudaStreamNonBlocking));
+    DP_CUDA(cudaEventCreateWithFlags(&b.fork, cudaEventDisableTiming));
+    DP_CUDA(cudaEventCreate(&b.start));
+    b.done.resize(b.ctx.size());
+    b.join.resize(b.ctx.size());
+    for (auto& e : b.done) DP_CUDA(cudaEventCreate(&e));
+    for (auto& e : b.join) DP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  b.free_graph();
+  b.gen.clear();
+  for (Ctx* c : b.ctx) {
+    ensure_ctl(*c);
+    b.gen.push_back(c->alloc_gen);
+  }
+  DP_CUDA(cudaStreamBeginCapture(b.s, cudaStreamCaptureModeRelaxed));
+  try {
+    DP_CUDA(cudaEventRecord(b.fork, b.s));
+    for (size_t i = 0; i < b.ctx.size(); ++i) {
+      Ctx& c = *b.ctx[i];
+      DP_CUDA(cudaStreamWaitEvent(c.stream, b.fork, 0));
+      capture_solve(c, b.cfg[i], (double*)c.work[W_U], (double*)c.work[W_P]);
+      DP_CUDA(cudaEventRecordWithFlags(b.done[i], c.stream, cudaEventRecordExternal));
+      DP_CUDA(cudaEventRecord(b.join[i], c.stream));
+      DP_CUDA(cudaStreamWaitEvent(b.s, b.join[i], 0));
+    }
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(b.s, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  DP_CUDA(cudaStreamEndCapture(b.s, &b.graph));
+  DP_CUDA(cudaGraphInstantiate(&b.exec, b.graph, 0));
+  DP_CUDA(cudaGraphUpload(b.exec, b.s));
+}
+
+// Launches the batch once; per-context results and completion times (ms from launch).
+// The graph holds the contexts' buffer addresses: a context whose multigrid or FP32
+// operator storage was reallocated since the capture (another precision or coarse
+// size solved on it meanwhile) makes the batch capture again first.
+void batch_run(Batch& b, std::vector<SolveResult>& res, std::vector<double>& done_ms) {
+  for (size_t i = 0; i < b.ctx.size(); ++i)
+    if (b.ctx[i]->alloc_gen != b.gen[i]) {
+      batch_build(b);
+      break;
+    }
+  for (size_t i = 0; i < b.ctx.size(); ++i) upload_params(*b.ctx[i], b.cfg[i], b.s);
+  DP_CUDA(cudaEventRecord(b.start, b.s));
+  DP_CUDA(cudaGraphLaunch(b.exec, b.s));
+  DP_CUDA(cudaStreamSynchronize(b.s));
+  res.resize(b.ctx.size());
+  done_ms.resize(b.ctx.size());
+  for (size_t i = 0; i < b.ctx.size(); ++i) {
+    collect_result(*b.ctx[i], b.cfg[i], b.s, res[i]);
+    float ms = 0.f;
+    DP_CUDA(cudaEventElapsedTime(&ms, b.start, b.done[i]));
+    done_ms[i] = ms;
+  }
 }
 
 }  // namespace dp

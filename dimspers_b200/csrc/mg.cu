@@ -473,6 +473,7 @@ template <>
 float* level_dinv<float>(MGLevel& L) { return L.dinv32; }
 
 void mg_free(Ctx& c) {
+  ++c.alloc_gen;
   for (size_t l = 0; l < c.mg.size(); ++l) {
     MGLevel& L = c.mg[l];
     if (l > 0) { cudaFree(L.K64); cudaFree(L.K32); }
@@ -666,8 +667,12 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
     c.mg_prec = prec;
     c.mg_coarse_max = o.coarse_max;
   }
-  // fine operator pointer
+  // fine operator pointer, apply tiles
   if (prec) c.mg[0].K32 = c.K32; else c.mg[0].K64 = c.K64;
+  for (MGLevel& L : c.mg) {
+    L.g.warps = o.apply_warps;
+    L.g.warps_t = o.apply_warps_t;
+  }
   // Galerkin coarse operators
   for (size_t l = 1; l < c.mg.size(); ++l) {
     MGLevel& Lf = c.mg[l - 1];

@@ -14,6 +14,8 @@ struct MGOptions {
   int max_levels = 16;
   int64_t coarse_max = 1024;// largest dense coarsest system
   int coarse_sweeps = 4;    // smoothing sweeps when the coarsest is not dense
+  int apply_warps = 4;      // tile of the element-by-element applies (Level::warps)
+  int apply_warps_t = 1;    // (Level::warps_t)
 };
 
 // Local node offsets (radial, angular) inside the cell for triangle type t.

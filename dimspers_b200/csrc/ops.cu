@@ -39,10 +39,24 @@ struct V2<float> { typedef float2 T; };
 template <>
 struct V2<double> { typedef double2 T; };
 
+// Element of this thread.  wt == 1: linear order (CTA = blockDim consecutive
+// elements).  wt > 1: the CTA is a tile of (blockDim/32/wt) x 16 radial cells by
+// wt theta columns; each warp still reads one contiguous 32-element block of K
+// (e = 2 (ir + ncr it) + t with ir = 16 m + lane/2, t = lane & 1).
+__device__ inline int tile_element(int ncr, int wt) {
+  if (wt == 1) return blockIdx.x * blockDim.x + threadIdx.x;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wr = (blockDim.x >> 5) / wt;       // warps along r
+  const int nbr = (ncr >> 4) / wr;              // CTAs along r
+  const int br = blockIdx.x % nbr, bt = blockIdx.x / nbr;
+  const int m = br * wr + w % wr, it = bt * wt + w / wr;
+  return 32 * m + 2 * ncr * it + lane;
+}
+
 template <typename Tm, typename Tv>
-__global__ void __launch_bounds__(128) k_apply_K(const Tm* __restrict__ K, const Tv* __restrict__ x,
-                                                 Tv* __restrict__ y, int nel, int ncr, int A, int B) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) k_apply_K(const Tm* __restrict__ K, const Tv* __restrict__ x,
+                                                 Tv* __restrict__ y, int nel, int ncr, int A, int B, int wt) {
+  const int e = tile_element(ncr, wt);
   if (e >= nel) return;
   typedef typename KVec<Tm>::V VT;
   constexpr int NV = KVec<Tm>::n;
@@ -91,12 +105,24 @@ __global__ void __launch_bounds__(128) k_apply_K(const Tm* __restrict__ K, const
   for (int k = 0; k < 6; ++k) atomic_add2(&y[2 * nd[k]], ye[2 * k], ye[2 * k + 1]);
 }
 
+// Grid of the tiled apply; the stacked tile only where it divides the lattice
+// exactly (ncr % (16 wr) == 0, nct % wt == 0), else the linear order.
+static void apply_tile(const Level& L, int& blocks, int& threads, int& wt) {
+  threads = 32 * L.warps;
+  wt = L.warps_t;
+  const int wr = L.warps / std::max(wt, 1);
+  if (wt > 1 && wr >= 1 && L.warps % wt == 0 && L.ncr % (16 * wr) == 0 && L.nct % wt == 0) {
+    blocks = (L.ncr / (16 * wr)) * (L.nct / wt);
+  } else {
+    wt = 1;
+    blocks = (int)div_up(L.nel, threads);
+  }
+}
+
 template <typename Tm, typename Tv>
 void launch_apply_K(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
   DP_CUDA(cudaMemsetAsync(y, 0, sizeof(Tv) * 2 * L.nnod, s));
-  ++g_klaunch;
-  k_apply_K<Tm, Tv><<<(int)div_up(L.nel, 128), 128, 0, s>>>(K, x, y, (int)L.nel, L.ncr, (int)L.A(), (int)L.B());
-  DP_LAUNCH_CHECK();
+  launch_apply_K_acc<Tm, Tv>(L, K, x, y, s);
 }
 template void launch_apply_K<double, double>(const Level&, const double*, const double*, double*, cudaStream_t);
 template void launch_apply_K<float, float>(const Level&, const float*, const float*, float*, cudaStream_t);
@@ -105,7 +131,9 @@ template void launch_apply_K<float, float>(const Level&, const float*, const flo
 template <typename Tm, typename Tv>
 void launch_apply_K_acc(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
   ++g_klaunch;
-  k_apply_K<Tm, Tv><<<(int)div_up(L.nel, 128), 128, 0, s>>>(K, x, y, (int)L.nel, L.ncr, (int)L.A(), (int)L.B());
+  int blocks, threads, wt;
+  apply_tile(L, blocks, threads, wt);
+  k_apply_K<Tm, Tv><<<blocks, threads, 0, s>>>(K, x, y, (int)L.nel, L.ncr, (int)L.A(), (int)L.B(), wt);
   DP_LAUNCH_CHECK();
 }
 template void launch_apply_K_acc<double, double>(const Level&, const double*, const double*, double*, cudaStream_t);

@@ -91,6 +91,16 @@ class GuessNet:
                                       C.c_float(lr), C.byref(loss)))
         return loss.value
 
+    def for_grid(self, nrg, ntg, max_batch=1, device=0):
+        """The same network (weights and normalisation) on another grid: the
+        layers are convolutions, so they apply unchanged at any resolution."""
+        net = GuessNet(nrg, ntg, self.channels, self.layers, self.dilations, max_batch, device)
+        net.set_params(self.get_params())
+        net.x_mean, net.x_std = self.x_mean, self.x_std
+        net.y_mean, net.y_std = self.y_mean, self.y_std
+        net.meta = dict(getattr(self, "meta", {}), nrg=nrg, ntg=ntg)
+        return net
+
     # ---- persistence -------------------------------------------------------------
     def save(self, path, extra=None):
         meta = dict(nrg=self.nrg, ntg=self.ntg, channels=self.channels, layers=self.layers,

@@ -93,6 +93,10 @@ typedef struct {
                               1 = M^-1 from the element mass blocks, what the
                               incomplete LDL^T of StokesPcCG_pardiso (:32,242)
                               gives for block-diagonal (discontinuous) M      */
+  int32_t apply_warps;     /* CTA of the element-by-element K applies, in warps
+                              (1, 2, 4, 8; 0 = default 4)                     */
+  int32_t apply_warps_t;   /* of those, warps stacked along theta (1 = linear
+                              element order; 0 = default 1)                   */
 } dp_solve_opts;
 
 typedef struct {
@@ -202,6 +206,22 @@ void dp_default_opts(dp_solve_opts* opts);
  * device share that array: calls that overlap on the GPU race.  The first call
  * on a device looks up the array's address; make it before any stream capture. */
 int dp_apply_K_noalloc(dp_ctx* ctx, const double* x, double* y);
+
+/* ---- batches of independent solves ---------------------------------------
+ * Independent problems (contexts of any resolution, all on one device) solved
+ * by ONE graph launch: the batch graph holds one branch per context with that
+ * context's whole solve, so small problems run side by side.  dp_batch_create
+ * prepares and captures (opts: one dp_solve_opts per context, NULL = defaults;
+ * no host loops); dp_batch_run recomputes each context's multigrid values for
+ * its current assembly, uploads the guesses (use_guess != 0), launches once
+ * and returns per-problem reports and completion times (ms from the launch).
+ * U, P, P_guess: arrays of n pointers (entries or whole arrays may be NULL for
+ * U and P). */
+typedef struct dp_batch dp_batch;
+int dp_batch_create(dp_ctx* const* ctxs, int32_t n, const dp_solve_opts* opts, dp_batch** out);
+int dp_batch_run(dp_batch* batch, double* const* P_guess, double* const* U, double* const* P, int32_t mem,
+                 dp_solve_report* reports, double* done_ms);
+void dp_batch_destroy(dp_batch* batch);
 
 /* ---- learned initial guess ----------------------------------------------
  * A small convolutional network on the polar grid of the half-resolution
