@@ -31,7 +31,8 @@ class SolveOpts(C.Structure):
                 ("max_refine", C.c_int32), ("host_loop", C.c_int32), ("block_jacobi", C.c_int32),
                 ("cheb_lo", C.c_double), ("cheb_hi", C.c_double), ("inner_relax", C.c_double),
                 ("coarse_max", C.c_int32), ("schur_pc", C.c_int32),
-                ("apply_warps", C.c_int32), ("apply_warps_t", C.c_int32)]
+                ("apply_warps", C.c_int32), ("apply_warps_t", C.c_int32),
+                ("launch_overlap", C.c_int32)]
 
 
 class SolveReport(C.Structure):

@@ -39,7 +39,7 @@ from .stokes import StokesContext, default_opts
 
 SIZES = ((32, 256), (64, 512), (128, 1024), (256, 2048))
 FAST = dict(precision=1, cheb_degree=3, cheb_lo=0.05, inner_rtol=1e-10, inner_relax=1e-4, schur_pc=1)
-TUNE_SPACE = dict(apply=((4, 1), (8, 1), (4, 4), (8, 2), (2, 2)), cheb_degree=(2, 3, 4), coarse_max=(256, 1024))
+TUNE_SPACE = dict(apply=((4, 1), (8, 1), (4, 4), (8, 2)), cheb_degree=(2, 3, 4), coarse_max=(1024, 1536))
 
 
 def tuning_key(ctx):
@@ -144,7 +144,7 @@ def tune_all(contexts, path=None, **kw):
         trials = autotune(c, **kw)
         table[key] = dict(trials[0], trials=len(trials), default=next(
             (t for t in trials if (t["apply_warps"], t["apply_warps_t"], t["cheb_degree"], t["coarse_max"]) ==
-             (4, 1, FAST["cheb_degree"], 1024)), None))
+             (4, 1, FAST["cheb_degree"], 1536)), None))
     if path:
         with open(path, "w") as f:
             json.dump(table, f, indent=1)

@@ -122,6 +122,8 @@ static SolveCfg make_cfg(const dp_solve_opts* o) {
   if (o->coarse_max > 0) cfg.mg.coarse_max = o->coarse_max;
   cfg.schur_pc = o->schur_pc;
   if (cfg.schur_pc != 0 && cfg.schur_pc != 1) throw BadArg("schur_pc must be 0 (lumped) or 1 (mass)");
+  if (o->launch_overlap != 0 && o->launch_overlap != 1) throw BadArg("launch_overlap must be 0 or 1");
+  cfg.launch_overlap = o->launch_overlap;
   if (o->apply_warps > 0) cfg.mg.apply_warps = o->apply_warps;
   if (o->apply_warps_t > 0) cfg.mg.apply_warps_t = o->apply_warps_t;
   {
@@ -315,9 +317,10 @@ void dp_default_opts(dp_solve_opts* o) {
   o->cheb_lo = 0.1;
   o->cheb_hi = 1.1;
   o->inner_relax = 0.0;
-  o->coarse_max = 1024;
+  o->coarse_max = 1536;
   o->apply_warps = 4;
   o->apply_warps_t = 1;
+  o->launch_overlap = 1;
 }
 
 const char* dp_status_string(int s) {
@@ -610,6 +613,7 @@ int dp_solve(dp_ctx* h, double* U, double* P, double* Ucart, const dp_solve_opts
     SolveResult res;
     if (cfg.host_loop) {
       const int64_t k0 = g_klaunch;
+      PdlScope pdl(cfg.launch_overlap);
       schur_pcg(c, cfg, dU, dP, res);
       res.launches = g_klaunch - k0;
     } else {

@@ -106,7 +106,7 @@ struct Ctx {
   int mg_degree = 3;            // Chebyshev steps in use
   int64_t mg_coarse_max = -1;   // coarse_max the hierarchy was built for
   int64_t alloc_gen = 0;        // bumped whenever buffers a captured graph may hold are freed
-  double* coarse_chol = nullptr;// dense Cholesky factor of the coarsest level
+  double* coarse_inv = nullptr; // coarsest level: work matrix, then its dense inverse (2 n^2)
   int64_t coarse_n = 0;
   int64_t* coarse_map = nullptr;// coarsest DOF -> dense index (-1 fixed)
 
@@ -148,6 +148,40 @@ struct CudaError {
   } while (0)
 
 #define DP_LAUNCH_CHECK() DP_CUDA(cudaGetLastError())
+
+// ---- programmatic dependent launch -------------------------------------------
+// The solver is a long chain of short kernels, many of them (coarse multigrid
+// levels, reductions, control) shorter than their own launch latency.  With
+// g_pdl set, klaunch gives each launch the programmatic-stream-serialization
+// attribute: the kernel may be scheduled while its predecessor is still
+// running, and waits in grid_dep_wait() (griddepcontrol.wait, which returns
+// once the predecessor grid has completed and its memory is visible) before it
+// touches memory.  Every kernel of the solve path calls grid_dep_wait() first,
+// so a launch with or without the attribute computes the same thing; without
+// the attribute the wait returns at once.
+__device__ __forceinline__ void grid_dep_wait() {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+
+inline thread_local int g_pdl = 0;
+
+template <typename... P, typename... A>
+inline void klaunch(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A... args) {
+  ++g_klaunch;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = g_pdl ? 1u : 0u;
+  DP_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<P>(args)...));
+}
 
 // ---- lattice helpers (host + device) ---------------------------------------
 // Constrained DOFs: u_r on both walls (free slip, boundary_conditions.jl:27-37)

@@ -53,6 +53,7 @@ __device__ inline double inner_rtol_now(const DevCtl* ctl, const double* scal, i
 
 __global__ void k_in_init(cudaGraphConditionalHandle h, DevCtl* ctl, const double* scal, int yy_slot, int irr_slot,
                           double* scal_w, int fp32, int relax) {
+  grid_dep_wait();
   const double yy = scal[yy_slot];
   const double rt = fp32 ? ctl->inner_rtol32 : inner_rtol_now(ctl, scal, relax);
   const double tol2 = rt * rt * yy;
@@ -63,6 +64,7 @@ __global__ void k_in_init(cudaGraphConditionalHandle h, DevCtl* ctl, const doubl
 }
 
 __global__ void k_in_check(cudaGraphConditionalHandle h, DevCtl* ctl, double* scal, int rz, int rzn, int irr, int fp32) {
+  grid_dep_wait();
   int it;
   double tol2;
   if (fp32) { it = ++ctl->in32_it; tol2 = ctl->in32_tol2; ctl->in32_total += 1; }
@@ -74,6 +76,7 @@ __global__ void k_in_check(cudaGraphConditionalHandle h, DevCtl* ctl, double* sc
 }
 
 __global__ void k_ref_init(cudaGraphConditionalHandle h, DevCtl* ctl, double* scal, int relax) {
+  grid_dep_wait();
   const double yy = scal[R_YY];
   const double rt = inner_rtol_now(ctl, scal, relax);
   ctl->ref_it = 0;
@@ -83,6 +86,7 @@ __global__ void k_ref_init(cudaGraphConditionalHandle h, DevCtl* ctl, double* sc
 }
 
 __global__ void k_ref_check(cudaGraphConditionalHandle h, DevCtl* ctl, const double* scal) {
+  grid_dep_wait();
   const int it = ++ctl->ref_it;
   ctl->ref_total += 1;
   const double rr = scal[R_RES2];
@@ -93,6 +97,7 @@ __global__ void k_ref_check(cudaGraphConditionalHandle h, DevCtl* ctl, const dou
 // ||r(P = 0)|| (learned-guess mode), so a guess shortens the solve only by
 // starting closer to the same absolute target.
 __global__ void k_outer_init(cudaGraphConditionalHandle h, DevCtl* ctl, const double* scal, int use_ref) {
+  grid_dep_wait();
   const double r0 = use_ref ? ctl->r0ref : sqrt(scal[S_RR]);
   ctl->r0 = r0;
   ctl->tol = r0 * ctl->rtol;
@@ -102,6 +107,7 @@ __global__ void k_outer_init(cudaGraphConditionalHandle h, DevCtl* ctl, const do
 }
 
 __global__ void k_outer_check(cudaGraphConditionalHandle h, DevCtl* ctl, const double* scal) {
+  grid_dep_wait();
   const int it = ++ctl->outer_it;
   const double qsq = scal[S_QSQ], rd = scal[S_RD], rn = sqrt(scal[S_RR]);
   unsigned go = 1u;
@@ -120,6 +126,7 @@ __global__ void k_outer_check(cudaGraphConditionalHandle h, DevCtl* ctl, const d
 // Learned-guess selection: keep the guess only if its initial Schur residual
 // is below the zero guess's (otherwise fall back to P = 0).
 __global__ void k_guess_select(DevCtl* ctl, double* scal) {
+  grid_dep_wait();
   const double rg = scal[S_RR], rz = scal[G_RZREF];
   const int use = rg < rz ? 1 : 0;
   ctl->guess_used = use;
@@ -132,6 +139,7 @@ __global__ void k_guess_select(DevCtl* ctl, double* scal) {
 __global__ void k_guess_apply(const DevCtl* ctl, double* __restrict__ U, const double* __restrict__ Uz,
                               double* __restrict__ r, const double* __restrict__ rz, double* __restrict__ P,
                               int64_t nU, int64_t nP) {
+  grid_dep_wait();
   if (ctl->guess_used) return;
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < nU) U[i] = Uz[i];
@@ -146,6 +154,7 @@ __global__ void k_guess_apply(const DevCtl* ctl, double* __restrict__ U, const d
 template <typename T>
 __global__ void k_pcg_dir_g(T* __restrict__ p, const T* __restrict__ z, T* __restrict__ Ap, int64_t n,
                             const double* scal, int rzn, int rz, const int* it) {
+  grid_dep_wait();
   const double beta = (*it == 0) ? 0.0 : scal[rzn] / scal[rz];
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) {
@@ -156,12 +165,14 @@ __global__ void k_pcg_dir_g(T* __restrict__ p, const T* __restrict__ z, T* __res
 
 // FP64 residual -> FP32 hierarchy input, scaled by 1/||r|| (keeps FP32 in range)
 __global__ void k_r_to_f32(const double* __restrict__ r, float* __restrict__ r32, const double* scal, int irr, int64_t n) {
+  grid_dep_wait();
   const double s = 1.0 / sqrt(scal[irr]);
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) r32[i] = (float)(s * r[i]);
 }
 __global__ void k_z_from_f32(const float* __restrict__ z32, double* __restrict__ z, const double* scal, int irr,
                              int64_t n) {
+  grid_dep_wait();
   const double s = sqrt(scal[irr]);
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) z[i] = s * (double)z32[i];
@@ -169,6 +180,7 @@ __global__ void k_z_from_f32(const float* __restrict__ z32, double* __restrict__
 // nodal block Jacobi with an inverse of another precision
 template <typename Td, typename Tv>
 __global__ void k_bj_mixed(const Td* __restrict__ dinv, const Tv* __restrict__ r, Tv* __restrict__ z, int64_t nnod) {
+  grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
   double z0, z1;
@@ -182,6 +194,7 @@ template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_pcg_upd_g(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
                                                             const T* __restrict__ Ap, int64_t n, double* scal, int rzn,
                                                             int pap, int irr, double* partial, unsigned int* counter) {
+  grid_dep_wait();
   const double alpha = scal[rzn] / scal[pap];
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
@@ -196,11 +209,13 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_upd_g(T* __restrict__ x, T*
 }
 
 __global__ void k_to_f32_scaled(const double* __restrict__ a, float* __restrict__ b, const double* scal, int64_t n) {
+  grid_dep_wait();
   const double s = 1.0 / sqrt(scal[R_RES2]);
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) b[i] = (float)(s * a[i]);
 }
 __global__ void k_add_f32_scaled(double* __restrict__ z, const float* __restrict__ e, const double* scal, int64_t n) {
+  grid_dep_wait();
   const double s = sqrt(scal[R_RES2]);
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) z[i] += s * (double)e[i];
@@ -284,8 +299,7 @@ static void emit_pcg(Ctx& c, const SolveCfg& cfg, const T* Kmat, const T* b, T* 
   if (f32) launch_dot_f(c, (const float*)b, (const float*)b, n, YY);
   else launch_dot(c, (const double*)b, (const double*)b, n, YY);
   cudaGraphConditionalHandle h = new_handle(c.stream);
-  ++g_klaunch;
-  k_in_init<<<1, 1, 0, c.stream>>>(h, ctl, c.scal, YY, IRR, c.scal, f32 ? 1 : 0, relax);
+  klaunch(k_in_init, 1, 1, 0, c.stream, h, ctl, c.scal, YY, IRR, c.scal, f32 ? 1 : 0, relax);
   DP_LAUNCH_CHECK();
   cudaGraph_t body = add_while(c.stream, h);
   const int* itp = f32 ? &ctl->in32_it : &ctl->in_it;
@@ -297,31 +311,25 @@ static void emit_pcg(Ctx& c, const SolveCfg& cfg, const T* Kmat, const T* b, T* 
       } else if (mixed) {
         float* r32 = (float*)c.work[W_F_R];
         float* z32 = (float*)c.work[W_F_Z];
-        ++g_klaunch;
-        k_r_to_f32<<<g_nb(n), 256, 0, c.stream>>>((const double*)r, r32, c.scal, IRR, n);
+        klaunch(k_r_to_f32, g_nb(n), 256, 0, c.stream, (const double*)r, r32, c.scal, IRR, n);
         mg_apply_f(c, r32, z32, cfg.mg);
-        ++g_klaunch;
-        k_z_from_f32<<<g_nb(n), 256, 0, c.stream>>>(z32, (double*)z, c.scal, IRR, n);
+        klaunch(k_z_from_f32, g_nb(n), 256, 0, c.stream, z32, (double*)z, c.scal, IRR, n);
       } else {
         mg_apply(c, (const double*)r, (double*)z, cfg.mg);
       }
     } else {
-      ++g_klaunch;
-      if (c.mg_prec == 1) k_bj_mixed<float, T><<<g_nb(L.nnod), 256, 0, c.stream>>>(c.mg[0].dinv32, r, z, L.nnod);
-      else k_bj_mixed<double, T><<<g_nb(L.nnod), 256, 0, c.stream>>>(c.mg[0].dinv64, r, z, L.nnod);
+      if (c.mg_prec == 1) klaunch(k_bj_mixed<float, T>, g_nb(L.nnod), 256, 0, c.stream, c.mg[0].dinv32, r, z, L.nnod);
+      else klaunch(k_bj_mixed<double, T>, g_nb(L.nnod), 256, 0, c.stream, c.mg[0].dinv64, r, z, L.nnod);
     }
     if (f32) launch_dot_f(c, (const float*)r, (const float*)z, n, RZN);
     else launch_dot(c, (const double*)r, (const double*)z, n, RZN);
-    ++g_klaunch;
-    k_pcg_dir_g<T><<<g_nb(n), 256, 0, c.stream>>>(p, z, Ap, n, c.scal, RZN, RZ, itp);
+    klaunch(k_pcg_dir_g<T>, g_nb(n), 256, 0, c.stream, p, z, Ap, n, c.scal, RZN, RZ, itp);
     launch_apply_K_acc<T, T>(L, Kmat, p, Ap, c.stream);
     if (f32) launch_dot_f(c, (const float*)p, (const float*)Ap, n, PAP);
     else launch_dot(c, (const double*)p, (const double*)Ap, n, PAP);
-    ++g_klaunch;
-    k_pcg_upd_g<T><<<red_grid(n), kRedThreads, 0, c.stream>>>(x, r, p, Ap, n, c.scal, RZN, PAP, IRR, c.partial,
+    klaunch(k_pcg_upd_g<T>, red_grid(n), kRedThreads, 0, c.stream, x, r, p, Ap, n, c.scal, RZN, PAP, IRR, c.partial,
                                                                c.counter);
-    ++g_klaunch;
-    k_in_check<<<1, 1, 0, c.stream>>>(h, ctl, c.scal, RZ, RZN, IRR, f32 ? 1 : 0);
+    klaunch(k_in_check, 1, 1, 0, c.stream, h, ctl, c.scal, RZ, RZN, IRR, f32 ? 1 : 0);
     DP_LAUNCH_CHECK();
   });
 }
@@ -342,23 +350,18 @@ static void emit_inner(Ctx& c, const SolveCfg& cfg, const double* b, double* x, 
   DP_CUDA(cudaMemcpyAsync(res, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, c.stream));
   launch_dot(c, b, b, n, R_YY);
   cudaGraphConditionalHandle h = new_handle(c.stream);
-  ++g_klaunch;
-  k_ref_init<<<1, 1, 0, c.stream>>>(h, ctl, c.scal, relax);
+  klaunch(k_ref_init, 1, 1, 0, c.stream, h, ctl, c.scal, relax);
   DP_LAUNCH_CHECK();
   cudaGraph_t body = add_while(c.stream, h);
   capture_body(c, body, depth, B_REF, [&] {
-    ++g_klaunch;
-    k_to_f32_scaled<<<g_nb(n), 256, 0, c.stream>>>(res, fb, c.scal, n);
+    klaunch(k_to_f32_scaled, g_nb(n), 256, 0, c.stream, res, fb, c.scal, n);
     emit_pcg<float>(c, cfg, c.K32, fb, fx, (float*)c.work[W_F_R], (float*)c.work[W_F_Z], (float*)c.work[W_F_P],
                     (float*)c.work[W_F_AP], depth + 1, 0);
-    ++g_klaunch;
-    k_add_f32_scaled<<<g_nb(n), 256, 0, c.stream>>>(x, fx, c.scal, n);
+    klaunch(k_add_f32_scaled, g_nb(n), 256, 0, c.stream, x, fx, c.scal, n);
     launch_apply_K<double, double>(c.fine, c.K64, x, res, c.stream);
-    ++g_klaunch;
-    k_residual<<<g_nb(n), 256, 0, c.stream>>>(b, res, n);
+    klaunch(k_residual, g_nb(n), 256, 0, c.stream, b, res, n);
     launch_dot(c, res, res, n, R_RES2);
-    ++g_klaunch;
-    k_ref_check<<<1, 1, 0, c.stream>>>(h, ctl, c.scal);
+    klaunch(k_ref_check, 1, 1, 0, c.stream, h, ctl, c.scal);
     DP_LAUNCH_CHECK();
   });
 }
@@ -382,92 +385,71 @@ static void emit_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
     double* rz = (double*)c.work[W_RLAST];
     emit_inner(c, cfg, c.F, Uz, 0, 0);
     launch_apply_GT(c, Uz, rz);
-    ++g_klaunch;
-    k_neg<<<g_nb(nP), 256, 0, c.stream>>>(rz, nP);
+    klaunch(k_neg, g_nb(nP), 256, 0, c.stream, rz, nP);
     launch_sum(c, rz, nP, S_SUMR);
-    ++g_klaunch;
-    k_sub_mean<<<g_nb(nP), 256, 0, c.stream>>>(rz, nP, c.scal + S_SUMR);
+    klaunch(k_sub_mean, g_nb(nP), 256, 0, c.stream, rz, nP, c.scal + S_SUMR);
     launch_dot(c, rz, rz, nP, G_RZREF);
   }
   // Rhs = F + G P ; U = K^-1 Rhs
   if (!cfg.use_guess) DP_CUDA(cudaMemsetAsync(P, 0, sizeof(double) * nP, c.stream));
   launch_apply_G(c, P, y);
-  ++g_klaunch;
-  k_add<<<g_nb(nU), 256, 0, c.stream>>>(c.F, y, rhs, nU);
+  klaunch(k_add, g_nb(nU), 256, 0, c.stream, c.F, y, rhs, nU);
   emit_inner(c, cfg, rhs, U, 0, 0);
   // r = -G^T U ; rm0space!(r) ; ||r0||
   launch_apply_GT(c, U, r);
-  ++g_klaunch;
-  k_neg<<<g_nb(nP), 256, 0, c.stream>>>(r, nP);
+  klaunch(k_neg, g_nb(nP), 256, 0, c.stream, r, nP);
   launch_sum(c, r, nP, S_SUMR);
-  ++g_klaunch;
-  k_sub_mean<<<g_nb(nP), 256, 0, c.stream>>>(r, nP, c.scal + S_SUMR);
+  klaunch(k_sub_mean, g_nb(nP), 256, 0, c.stream, r, nP, c.scal + S_SUMR);
   launch_dot(c, r, r, nP, S_RR);
   if (cfg.use_guess == 2) {
-    ++g_klaunch;
-    k_guess_select<<<1, 1, 0, c.stream>>>(ctl, c.scal);
-    ++g_klaunch;
-    k_guess_apply<<<g_nb(std::max(nU, nP)), 256, 0, c.stream>>>(ctl, U, (const double*)c.work[W_UC], r,
+    klaunch(k_guess_select, 1, 1, 0, c.stream, ctl, c.scal);
+    klaunch(k_guess_apply, g_nb(std::max(nU, nP)), 256, 0, c.stream, ctl, U, (const double*)c.work[W_UC], r,
                                                                   (const double*)c.work[W_RLAST], P, nU, nP);
   }
   // d = r .* pc (or M^-1 r) ; q = d
   if (cfg.schur_pc == 1) {
-    ++g_klaunch;
-    k_mass_blk<<<g_nb(L.nel), 256, 0, c.stream>>>(r, c.Minv, d, (int)L.nel);
+    klaunch(k_mass_blk, g_nb(L.nel), 256, 0, c.stream, r, c.Minv, d, (int)L.nel);
   } else {
-    ++g_klaunch;
-    k_mul_into<<<g_nb(nP), 256, 0, c.stream>>>(r, c.pc, d, nP);
+    klaunch(k_mul_into, g_nb(nP), 256, 0, c.stream, r, c.pc, d, nP);
   }
   DP_CUDA(cudaMemcpyAsync(q, d, sizeof(double) * nP, cudaMemcpyDeviceToDevice, c.stream));
   launch_sum(c, q, nP, S_SUMQ);
   cudaGraphConditionalHandle h = new_handle(c.stream);
-  ++g_klaunch;
-  k_outer_init<<<1, 1, 0, c.stream>>>(h, ctl, c.scal, cfg.use_guess == 2 ? 1 : 0);
+  klaunch(k_outer_init, 1, 1, 0, c.stream, h, ctl, c.scal, cfg.use_guess == 2 ? 1 : 0);
   DP_LAUNCH_CHECK();
   cudaGraph_t body = add_while(c.stream, h);
   capture_body(c, body, 0, B_OUTER, [&] {
-    ++g_klaunch;
-    k_q_center_rd<<<red_grid(nP), kRedThreads, 0, c.stream>>>(q, r, d, nP, c.scal, c.partial, c.counter);
+    klaunch(k_q_center_rd, red_grid(nP), kRedThreads, 0, c.stream, q, r, d, nP, c.scal, c.partial, c.counter);
     launch_apply_G(c, q, y);
     emit_inner(c, cfg, y, z, 1, cfg.inner_relax > 0.0 ? 1 : 0);
     launch_apply_GT(c, z, Sq);
     launch_dot(c, q, Sq, nP, S_QSQ);
-    ++g_klaunch;
-    k_schur_update_p<<<red_grid(nP), kRedThreads, 0, c.stream>>>(P, r, rlast, q, Sq, nP, c.scal, c.partial, c.counter);
-    ++g_klaunch;
-    k_axpy_slot<<<g_nb(nU), 256, 0, c.stream>>>(U, z, nU, c.scal);
-    ++g_klaunch;
+    klaunch(k_schur_update_p, red_grid(nP), kRedThreads, 0, c.stream, P, r, rlast, q, Sq, nP, c.scal, c.partial, c.counter);
+    klaunch(k_axpy_slot, g_nb(nU), 256, 0, c.stream, U, z, nU, c.scal);
     if (cfg.schur_pc == 1)
-      k_schur_center_blk<<<red_grid(L.nel), kRedThreads, 0, c.stream>>>(r, rlast, c.Minv, d, (int)L.nel, c.scal,
+      klaunch(k_schur_center_blk, red_grid(L.nel), kRedThreads, 0, c.stream, r, rlast, c.Minv, d, (int)L.nel, c.scal,
                                                                          c.partial, c.counter);
     else
-      k_schur_center<<<red_grid(nP), kRedThreads, 0, c.stream>>>(r, rlast, c.pc, d, nP, c.scal, c.partial, c.counter);
-    ++g_klaunch;
-    k_q_update<<<red_grid(nP), kRedThreads, 0, c.stream>>>(q, d, nP, c.scal, c.partial, c.counter);
-    ++g_klaunch;
-    k_outer_check<<<1, 1, 0, c.stream>>>(h, ctl, c.scal);
+      klaunch(k_schur_center, red_grid(nP), kRedThreads, 0, c.stream, r, rlast, c.pc, d, nP, c.scal, c.partial, c.counter);
+    klaunch(k_q_update, red_grid(nP), kRedThreads, 0, c.stream, q, d, nP, c.scal, c.partial, c.counter);
+    klaunch(k_outer_check, 1, 1, 0, c.stream, h, ctl, c.scal);
     DP_LAUNCH_CHECK();
   });
   // diagnostics on the raw solution
   launch_apply_K<double, double>(L, c.K64, U, rhs, c.stream);
   launch_apply_G(c, P, y);
-  ++g_klaunch;
-  k_add<<<g_nb(nU), 256, 0, c.stream>>>(c.F, y, y, nU);
-  ++g_klaunch;
-  k_residual<<<g_nb(nU), 256, 0, c.stream>>>(y, rhs, nU);
+  klaunch(k_add, g_nb(nU), 256, 0, c.stream, c.F, y, y, nU);
+  klaunch(k_residual, g_nb(nU), 256, 0, c.stream, y, rhs, nU);
   launch_dot(c, rhs, rhs, nU, S_TMP);
   launch_dot(c, c.F, c.F, nU, S_TMP2);
   launch_apply_GT(c, U, Sq);
   launch_sum(c, Sq, nP, S_SUMR);
-  ++g_klaunch;
-  k_sub_mean<<<g_nb(nP), 256, 0, c.stream>>>(Sq, nP, c.scal + S_SUMR);
+  klaunch(k_sub_mean, g_nb(nP), 256, 0, c.stream, Sq, nP, c.scal + S_SUMR);
   launch_dot(c, Sq, Sq, nP, G_TMP3);
   if (cfg.remove_rotation) {
-    ++g_klaunch;
-    k_rot_integrals<<<red_grid(L.nel), kRedThreads, 0, c.stream>>>(U, c.rho_lat, c.theta_lat, c.r_lat, (int)L.nel, L.ncr,
+    klaunch(k_rot_integrals, red_grid(L.nel), kRedThreads, 0, c.stream, U, c.rho_lat, c.theta_lat, c.r_lat, (int)L.nel, L.ncr,
                                                                    (int)L.A(), (int)L.B(), c.scal, c.partial, c.counter);
-    ++g_klaunch;
-    k_rot_remove<<<g_nb(L.nnod), 256, 0, c.stream>>>(U, c.r_lat, L.nnod, c.scal);
+    klaunch(k_rot_remove, g_nb(L.nnod), 256, 0, c.stream, U, c.r_lat, L.nnod, c.scal);
   }
   DP_LAUNCH_CHECK();
 }
@@ -477,7 +459,8 @@ static int64_t graph_key(const SolveCfg& cfg, const Ctx& c) {
          ((int64_t)cfg.remove_rotation << 5) | ((int64_t)c.mg_degree << 6) | ((int64_t)c.mg.size() << 10) |
          ((int64_t)(cfg.inner_relax > 0.0) << 15) | ((int64_t)c.mg_prec << 16) | ((int64_t)cfg.schur_pc << 18) |
          ((int64_t)cfg.mg.block_jacobi << 20) | ((int64_t)(c.coarse_n > 0) << 21) |
-         ((int64_t)cfg.mg.apply_warps << 24) | ((int64_t)cfg.mg.apply_warps_t << 28);
+         ((int64_t)cfg.mg.apply_warps << 24) | ((int64_t)cfg.mg.apply_warps_t << 28) |
+         ((int64_t)cfg.launch_overlap << 32);
 }
 
 void graph_free(Ctx& c) {
@@ -499,6 +482,7 @@ static void ensure_ctl(Ctx& c) {
 // Captures the solve of c (on c.stream, which may be part of an enclosing
 // capture) and records its kernel-count bookkeeping.
 static void capture_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
+  PdlScope pdl(cfg.launch_overlap);
   const int64_t start = g_klaunch;
   c.cap_nested = 0;
   emit_solve(c, cfg, U, P);

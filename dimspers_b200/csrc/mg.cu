@@ -15,8 +15,8 @@
 // followed by the coarse free-slip mask.  This keeps every level in the same
 // packed element-by-element form as the fine level.
 // Smoother: Chebyshev polynomial in D^-1 A (point Jacobi), bounds from a
-// 10-step CG-Lanczos estimate of lambda_max.  Coarsest level: dense Cholesky,
-// inverted once per setup and applied as a dense mat-vec.
+// 10-step CG-Lanczos estimate of lambda_max.  Coarsest level: assembled densely,
+// inverted once per setup by Gauss-Jordan sweeps and applied as a dense mat-vec.
 #include <algorithm>
 #include <cmath>
 #include <stdexcept>
@@ -150,6 +150,7 @@ void upload_mg_constants() {
 template <typename T>
 __global__ void k_galerkin(const T* __restrict__ Kf, T* __restrict__ Kc, int nelc, int ncrc, int nctc, int nelf,
                            int ncrf, int pin) {
+  grid_dep_wait();
   const int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (gid >= (int64_t)nelc * kKe) return;
   const int E = (int)(gid % nelc);
@@ -196,6 +197,7 @@ __global__ void k_galerkin(const T* __restrict__ Kf, T* __restrict__ Kc, int nel
 // ---- nodal 2x2 diagonal blocks and their inverses ----------------------------
 template <typename T>
 __global__ void k_diag_blocks(const T* __restrict__ K, double* __restrict__ diag, int nel, int ncr, int A, int B) {
+  grid_dep_wait();
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nel) return;
   int nd[6];
@@ -213,6 +215,7 @@ __global__ void k_diag_blocks(const T* __restrict__ K, double* __restrict__ diag
 template <typename T>
 __global__ void k_block_invert(const double* __restrict__ diag, T* __restrict__ dinv, int64_t nnod, int A, int pin,
                                int block) {
+  grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
   const int a = (int)(n % A), b = (int)(n / A);
@@ -278,6 +281,7 @@ __device__ inline void fine_node_weights(int a, int b, int ncrc, int Ac, int Bc,
 template <typename T>
 __global__ void k_prolong_add(const T* __restrict__ xc, T* __restrict__ xf, T* __restrict__ zb, int Af, int Bf,
                               int ncrc, int Ac, int Bc, int pin) {
+  grid_dep_wait();
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= Af * Bf) return;
   const int a = n % Af, b = n / Af;
@@ -299,29 +303,59 @@ __global__ void k_prolong_add(const T* __restrict__ xc, T* __restrict__ xf, T* _
 }
 
 // bc = P^T (r - t) per coarse node (gather over the class stencil); constrained
-// DOFs of either level are excluded.
+// DOFs of either level are excluded.  blockIdx.y is the parity class, so the
+// stencil reads are uniform across a warp (constant-cache broadcast), and the
+// stencil loop is unrolled with its loads predicated rather than branched, so
+// a thread keeps several gathers in flight.
+// first != 0 also takes the coarse level's first Chebyshev step from x = 0
+// (the work of k_cheb_first): rc = bc, dc = xc = coef[0] D^-1 bc, tc = 0.
 template <typename T>
-__global__ void k_restrict_g(const T* __restrict__ r, const T* __restrict__ t, T* __restrict__ bc, int Af, int Bf,
-                             int Ac, int Bc, int pin) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= Ac * Bc) return;
-  const int ac = n % Ac, bcn = n / Ac;
-  const int cls = (ac & 1) | ((bcn & 1) << 1);
+__global__ void __launch_bounds__(256) k_restrict_g(const T* __restrict__ r, const T* __restrict__ t, T* __restrict__ bc,
+                                                    int Af, int Bf, int Ac, int Bc, int pin, int first,
+                                                    const T* __restrict__ dinv_c, T* __restrict__ xc, T* __restrict__ rc,
+                                                    T* __restrict__ dc, T* __restrict__ tc,
+                                                    const double* __restrict__ coef_c) {
+  grid_dep_wait();
+  const int cls = blockIdx.y;
+  const int pa = cls & 1, pb = cls >> 1;
+  const int nA = (Ac - pa + 1) >> 1;  // coarse a = pa, pa + 2, ... <= Ac - 1
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nA * (Bc >> 1)) return;
+  const int ac = 2 * (idx % nA) + pa, bcn = 2 * (idx / nA) + pb;
+  typedef typename V2<T>::T X2;
+  const X2* r2 = reinterpret_cast<const X2*>(r);
+  const X2* t2 = reinterpret_cast<const X2*>(t);
   const int m = c_rtab.n[cls];
   double s0 = 0.0, s1 = 0.0;
+#pragma unroll 8
   for (int j = 0; j < m; ++j) {
     const int a = 2 * ac + c_rtab.da[cls][j];
-    if (a < 0 || a >= Af) continue;
     int b = 2 * bcn + c_rtab.db[cls][j];
-    if (b < 0) b += Bf;
-    if (b >= Bf) b -= Bf;
-    const int f = a + Af * b;
+    b += (b < 0) ? Bf : 0;
+    b -= (b >= Bf) ? Bf : 0;
+    const bool in = a >= 0 && a < Af;
+    const int f = in ? a + Af * b : 0;
+    const X2 rv = r2[f], tv = t2[f];
     const double w = c_rtab.w[cls][j];
-    if (!dof_fixed(a, b, 0, Af - 1, pin)) s0 += w * ((double)r[2 * f] - (double)t[2 * f]);
-    if (!dof_fixed(a, b, 1, Af - 1, pin)) s1 += w * ((double)r[2 * f + 1] - (double)t[2 * f + 1]);
+    const double w0 = (in && !dof_fixed(a, b, 0, Af - 1, pin)) ? w : 0.0;
+    const double w1 = (in && !dof_fixed(a, b, 1, Af - 1, pin)) ? w : 0.0;
+    s0 += w0 * ((double)rv.x - (double)tv.x);
+    s1 += w1 * ((double)rv.y - (double)tv.y);
   }
-  bc[2 * n] = dof_fixed(ac, bcn, 0, Ac - 1, pin) ? (T)0 : (T)s0;
-  bc[2 * n + 1] = dof_fixed(ac, bcn, 1, Ac - 1, pin) ? (T)0 : (T)s1;
+  const int n = ac + Ac * bcn;
+  const double b0 = dof_fixed(ac, bcn, 0, Ac - 1, pin) ? 0.0 : s0;
+  const double b1 = dof_fixed(ac, bcn, 1, Ac - 1, pin) ? 0.0 : s1;
+  bc[2 * n] = (T)b0;
+  bc[2 * n + 1] = (T)b1;
+  if (first) {
+    const double it = coef_c[0];
+    double z0, z1;
+    bj_apply<T>(dinv_c, n, b0, b1, z0, z1);
+    tc[2 * n] = (T)0; tc[2 * n + 1] = (T)0;
+    rc[2 * n] = (T)b0; rc[2 * n + 1] = (T)b1;
+    dc[2 * n] = (T)(it * z0); dc[2 * n + 1] = (T)(it * z1);
+    xc[2 * n] = (T)(it * z0); xc[2 * n + 1] = (T)(it * z1);
+  }
 }
 
 // ---- Chebyshev smoother vector steps (per node, coefficients read from device) --
@@ -331,6 +365,7 @@ template <typename T>
 __global__ void k_cheb_first(const T* __restrict__ b, const T* __restrict__ dinv, T* __restrict__ x,
                              T* __restrict__ r, T* __restrict__ d, T* __restrict__ t, const double* __restrict__ coef,
                              int64_t nnod) {
+  grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
   t[2 * n] = (T)0; t[2 * n + 1] = (T)0;
@@ -347,6 +382,7 @@ template <typename T>
 __global__ void k_cheb_first_x(const T* __restrict__ b, const T* __restrict__ dinv, T* __restrict__ x,
                                T* __restrict__ r, T* __restrict__ d, T* __restrict__ t,
                                const double* __restrict__ coef, int64_t nnod) {
+  grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
   t[2 * n] = (T)0; t[2 * n + 1] = (T)0;
@@ -362,6 +398,7 @@ __global__ void k_cheb_first_x(const T* __restrict__ b, const T* __restrict__ di
 template <typename T>
 __global__ void k_cheb_step(T* __restrict__ Ad, const T* __restrict__ dinv, T* __restrict__ x,
                             T* __restrict__ r, T* __restrict__ d, const double* __restrict__ coef, int64_t nnod) {
+  grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
   const double c1 = coef[0], c2 = coef[1];
@@ -376,12 +413,14 @@ __global__ void k_cheb_step(T* __restrict__ Ad, const T* __restrict__ dinv, T* _
 }
 template <typename T>
 __global__ void k_sub(const T* __restrict__ b, T* __restrict__ r, int64_t n) {  // r = b - r
+  grid_dep_wait();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) r[i] = b[i] - r[i];
 }
 // z = D^-1 r (nodal blocks)
 template <typename T>
 __global__ void k_bj(const T* __restrict__ dinv, const T* __restrict__ r, T* __restrict__ z, int64_t nnod) {
+  grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
   double z0, z1;
@@ -393,6 +432,7 @@ __global__ void k_bj(const T* __restrict__ dinv, const T* __restrict__ r, T* __r
 // ---- coarse dense solve --------------------------------------------------------
 template <typename T>
 __global__ void k_dense_assemble(const T* __restrict__ K, double* __restrict__ D, int nel, int ncr, int A, int B, int n) {
+  grid_dep_wait();
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nel) return;
   int nd[6];
@@ -406,54 +446,48 @@ __global__ void k_dense_assemble(const T* __restrict__ K, double* __restrict__ D
     }
 }
 
-// identity on fixed (zero) rows, then in-place Cholesky (lower) in one CTA
-__global__ void k_dense_cholesky(double* __restrict__ D, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x)
-    if (D[(size_t)i * n + i] == 0.0) D[(size_t)i * n + i] = 1.0;
-  __syncthreads();
-  for (int k = 0; k < n; ++k) {
-    if (threadIdx.x == 0) D[(size_t)k * n + k] = sqrt(D[(size_t)k * n + k]);
-    __syncthreads();
-    const double dk = D[(size_t)k * n + k];
-    for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x) D[(size_t)i * n + k] /= dk;
-    __syncthreads();
-    const int m = n - k - 1;
-    for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
-      const int i = k + 1 + idx / m, j = k + 1 + idx % m;
-      if (j <= i) D[(size_t)i * n + j] -= D[(size_t)i * n + k] * D[(size_t)j * n + k];
-    }
-    __syncthreads();
-  }
+// Identity on the diagonal of fixed (all-zero) rows, so the matrix stays SPD.
+__global__ void k_dense_fix_diag(double* __restrict__ D, int n) {
+  grid_dep_wait();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && D[(size_t)i * n + i] == 0.0) D[(size_t)i * n + i] = 1.0;
 }
 
-// Inverse from the Cholesky factor: column c of A^-1 by forward + back substitution.
-__global__ void k_dense_inverse(const double* __restrict__ L, double* __restrict__ Inv, double* __restrict__ tmp, int n) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n) return;
-  double* y = tmp + (size_t)c * n;
-  for (int i = 0; i < n; ++i) {
-    double s = (i == c) ? 1.0 : 0.0;
-    for (int j = 0; j < i; ++j) s -= L[(size_t)i * n + j] * y[j];
-    y[i] = s / L[(size_t)i * n + i];
-  }
-  for (int i = n - 1; i >= 0; --i) {
-    double s = y[i];
-    for (int j = i + 1; j < n; ++j) s -= L[(size_t)j * n + i] * y[j];
-    y[i] = s / L[(size_t)i * n + i];
-  }
-  for (int i = 0; i < n; ++i) Inv[(size_t)i * n + c] = y[i];
+// One Gauss-Jordan pivot step of the in-place inversion, ping-pong (A -> B):
+// with p = A_kk,  B_kk = 1/p,  B_kj = A_kj/p,  B_ik = -A_ik/p,
+// B_ij = A_ij - A_ik A_kj / p.  After the n steps B = A^-1.  The matrix is
+// SPD, so the pivots are positive and no pivoting is needed.  Threads run along
+// rows, so every step reads and writes the matrix with coalesced accesses.
+__global__ void k_gauss_jordan_step(const double* __restrict__ A, double* __restrict__ B, int n, int k) {
+  grid_dep_wait();
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)n * n) return;
+  const int i = (int)(idx / n), j = (int)(idx % n);
+  const double ip = 1.0 / A[(size_t)k * n + k];
+  double v;
+  if (i == k) v = (j == k) ? ip : A[(size_t)k * n + j] * ip;
+  else if (j == k) v = -A[(size_t)i * n + k] * ip;
+  else v = A[idx] - A[(size_t)i * n + k] * A[(size_t)k * n + j] * ip;
+  B[idx] = v;
 }
 
+// x = Inv b, one CTA per row: each thread reads a few entries of the row (all
+// loads in flight at once), then a block reduction.
 template <typename T>
-__global__ void k_dense_apply(const double* __restrict__ Inv, const T* __restrict__ b, T* __restrict__ x, int n) {
-  const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (row >= n) return;
+__global__ void __launch_bounds__(128) k_dense_apply(const double* __restrict__ Inv, const T* __restrict__ b,
+                                                     T* __restrict__ x, int n) {
+  grid_dep_wait();
+  const int row = blockIdx.x;
+  const double* a = Inv + (size_t)row * n;
   double s = 0.0;
-  for (int j = lane; j < n; j += 32) s += Inv[(size_t)row * n + j] * (double)b[j];
+#pragma unroll 4
+  for (int j = threadIdx.x; j < n; j += 128) s += a[j] * (double)b[j];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  if (lane == 0) x[row] = (T)s;
+  __shared__ double part[4];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) x[row] = (T)(part[0] + part[1] + part[2] + part[3]);
 }
 
 // ---- host side ---------------------------------------------------------------
@@ -481,8 +515,8 @@ void mg_free(Ctx& c) {
     cudaFree(L.x); cudaFree(L.b); cudaFree(L.r); cudaFree(L.d); cudaFree(L.t);
   }
   c.mg.clear();
-  cudaFree(c.coarse_chol);
-  c.coarse_chol = nullptr;
+  cudaFree(c.coarse_inv);
+  c.coarse_inv = nullptr;
   c.coarse_n = 0;
   c.mg_prec = -1;
 }
@@ -527,6 +561,7 @@ void dot_level<float>(Ctx& c, const float* a, const float* b, int64_t n, int slo
 
 template <typename T>
 __global__ void k_fill_pattern(T* v, int64_t n, int A, int pin) {
+  grid_dep_wait();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   // deterministic pseudo-random start vector, zero on fixed DOFs
@@ -544,6 +579,7 @@ __global__ void k_fill_pattern(T* v, int64_t n, int A, int pin) {
 template <typename T>
 __global__ void k_pcg_vec(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p, const T* __restrict__ Ap,
                           const T* __restrict__ dinv, T* __restrict__ z, double alpha, int64_t nnod) {
+  grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
   double rr[2];
@@ -560,6 +596,7 @@ __global__ void k_pcg_vec(T* __restrict__ x, T* __restrict__ r, const T* __restr
 }
 template <typename T>
 __global__ void k_xpby(const T* __restrict__ z, T* __restrict__ p, double beta, int64_t n) {
+  grid_dep_wait();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) p[i] = z[i] + (T)(beta * (double)p[i]);
 }
@@ -571,10 +608,8 @@ static double estimate_lmax(Ctx& c, MGLevel& L) {
   T* x = (T*)L.x; T* r = (T*)L.r; T* p = (T*)L.d; T* z = (T*)L.b; T* Ap = (T*)L.t;
   const T* dinv = level_dinv<T>(L);
   DP_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * n, c.stream));
-  ++g_klaunch;
-  k_fill_pattern<T><<<tpb(n), 256, 0, c.stream>>>(r, n, (int)L.g.A(), L.g.pin);
-  ++g_klaunch;
-  k_bj<T><<<tpb(L.g.nnod), 256, 0, c.stream>>>(dinv, r, z, L.g.nnod);
+  klaunch(k_fill_pattern<T>, tpb(n), 256, 0, c.stream, r, n, (int)L.g.A(), L.g.pin);
+  klaunch(k_bj<T>, tpb(L.g.nnod), 256, 0, c.stream, dinv, r, z, L.g.nnod);
   DP_CUDA(cudaMemcpyAsync(p, z, sizeof(T) * n, cudaMemcpyDeviceToDevice, c.stream));
   dot_level<T>(c, r, z, n, 20);
   DP_CUDA(cudaMemcpyAsync(c.h_scal + 20, c.scal + 20, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
@@ -590,8 +625,7 @@ static double estimate_lmax(Ctx& c, MGLevel& L) {
     const double pAp = c.h_scal[21];
     if (!(pAp > 0.0)) break;
     const double alpha = rz / pAp;
-    ++g_klaunch;
-    k_pcg_vec<T><<<tpb(L.g.nnod), 256, 0, c.stream>>>(x, r, p, Ap, dinv, z, alpha, L.g.nnod);
+    klaunch(k_pcg_vec<T>, tpb(L.g.nnod), 256, 0, c.stream, x, r, p, Ap, dinv, z, alpha, L.g.nnod);
     dot_level<T>(c, r, z, n, 20);
     DP_CUDA(cudaMemcpyAsync(c.h_scal + 20, c.scal + 20, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     DP_CUDA(cudaStreamSynchronize(c.stream));
@@ -601,8 +635,7 @@ static double estimate_lmax(Ctx& c, MGLevel& L) {
     betas.push_back(beta);
     rz = rz_new;
     if (!(rz > 0.0)) break;
-    ++g_klaunch;
-    k_xpby<T><<<tpb(n), 256, 0, c.stream>>>(z, p, beta, n);
+    klaunch(k_xpby<T>, tpb(n), 256, 0, c.stream, z, p, beta, n);
   }
   DP_LAUNCH_CHECK();
   const int m = (int)alphas.size();
@@ -660,7 +693,7 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
     }
     c.coarse_n = 2 * c.mg.back().g.nnod;
     if (c.coarse_n <= o.coarse_max) {
-      DP_CUDA(cudaMalloc(&c.coarse_chol, sizeof(double) * c.coarse_n * c.coarse_n * 3));
+      DP_CUDA(cudaMalloc(&c.coarse_inv, sizeof(double) * c.coarse_n * c.coarse_n * 2));
     } else {
       c.coarse_n = 0;
     }
@@ -678,8 +711,7 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
     MGLevel& Lf = c.mg[l - 1];
     MGLevel& Lc = c.mg[l];
     const int64_t nthreads = Lc.g.nel * kKe;
-    ++g_klaunch;
-    k_galerkin<T><<<(int)div_up(nthreads, 128), 128, 0, c.stream>>>(level_K<T>(Lf), level_K<T>(Lc), (int)Lc.g.nel,
+    klaunch(k_galerkin<T>, (int)div_up(nthreads, 128), 128, 0, c.stream, level_K<T>(Lf), level_K<T>(Lc), (int)Lc.g.nel,
                                                                       Lc.g.ncr, Lc.g.nct, (int)Lf.g.nel, Lf.g.ncr,
                                                                       Lc.g.pin);
     DP_LAUNCH_CHECK();
@@ -691,11 +723,9 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
   for (size_t l = 0; l < c.mg.size(); ++l) {
     MGLevel& L = c.mg[l];
     DP_CUDA(cudaMemsetAsync(diag, 0, sizeof(double) * 3 * L.g.nnod, c.stream));
-    ++g_klaunch;
-    k_diag_blocks<T><<<(int)div_up(L.g.nel, 128), 128, 0, c.stream>>>(level_K<T>(L), diag, (int)L.g.nel, L.g.ncr,
+    klaunch(k_diag_blocks<T>, (int)div_up(L.g.nel, 128), 128, 0, c.stream, level_K<T>(L), diag, (int)L.g.nel, L.g.ncr,
                                                                        (int)L.g.A(), (int)L.g.B());
-    ++g_klaunch;
-    k_block_invert<T><<<tpb(L.g.nnod), 256, 0, c.stream>>>(diag, level_dinv<T>(L), L.g.nnod, (int)L.g.A(), L.g.pin,
+    klaunch(k_block_invert<T>, tpb(L.g.nnod), 256, 0, c.stream, diag, level_dinv<T>(L), L.g.nnod, (int)L.g.A(), L.g.pin,
                                                             o.block_jacobi);
     DP_LAUNCH_CHECK();
     const bool is_coarsest_direct = (l + 1 == c.mg.size()) && c.coarse_n > 0;
@@ -723,17 +753,17 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
   if (c.coarse_n > 0) {
     MGLevel& L = c.mg.back();
     const int n = (int)c.coarse_n;
-    double* D = c.coarse_chol;
+    double* D = c.coarse_inv;
     double* Inv = D + (size_t)n * n;
-    double* tmp = Inv + (size_t)n * n;
     DP_CUDA(cudaMemsetAsync(D, 0, sizeof(double) * n * n, c.stream));
-    ++g_klaunch;
-    k_dense_assemble<T><<<(int)div_up(L.g.nel, 128), 128, 0, c.stream>>>(level_K<T>(L), D, (int)L.g.nel, L.g.ncr,
+    klaunch(k_dense_assemble<T>, (int)div_up(L.g.nel, 128), 128, 0, c.stream, level_K<T>(L), D, (int)L.g.nel, L.g.ncr,
                                                                           (int)L.g.A(), (int)L.g.B(), n);
-    ++g_klaunch;
-    k_dense_cholesky<<<1, 1024, 0, c.stream>>>(D, n);
-    ++g_klaunch;
-    k_dense_inverse<<<(int)div_up(n, 64), 64, 0, c.stream>>>(D, Inv, tmp, n);
+    klaunch(k_dense_fix_diag, (int)div_up(n, 256), 256, 0, c.stream, D, n);
+    double* buf[2] = {D, Inv};
+    const int blocks = (int)div_up((int64_t)n * n, 256);
+    for (int k = 0; k < n; ++k) klaunch(k_gauss_jordan_step, blocks, 256, 0, c.stream, buf[k & 1], buf[(k + 1) & 1], n, k);
+    // step k writes buf[(k + 1) & 1]: for even n the inverse ends in D
+    if (!(n & 1)) DP_CUDA(cudaMemcpyAsync(Inv, D, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, c.stream));
     DP_LAUNCH_CHECK();
   }
 }
@@ -743,48 +773,48 @@ void mg_setup(Ctx& c, int precision, const MGOptions& o) {
   else mg_setup_t<double>(c, o);
 }
 
-// Chebyshev smoothing of A x = b on level L.  x_zero: start from x = 0.
-// Otherwise L.r must hold zeros on entry (the prolongation zeroes it).  The
-// recurrence coefficients live in L.cheb on the device, so this sequence is
-// the same for every assembly and is captured once into the solve graph.
+// Chebyshev smoothing of A x = b on level L.  mode 0: start from x = 0;
+// mode 1: start from x = 0 with the first step already taken (fused into the
+// restriction that produced b); mode 2: start from the given x, with L.r
+// holding zeros on entry (the prolongation zeroes it).  The recurrence
+// coefficients live in L.cheb on the device, so this sequence is the same for
+// every assembly and is captured once into the solve graph.
 // On exit r = b - A (x - d_last), i.e. the true residual is r - A d_last.
 template <typename T>
-static void chebyshev(Ctx& c, MGLevel& L, const T* b, T* x, bool x_zero) {
+static void chebyshev(Ctx& c, MGLevel& L, const T* b, T* x, int mode) {
   const int64_t nn = L.g.nnod;
   T* r = (T*)L.r; T* d = (T*)L.d; T* Ad = (T*)L.t;
   const T* dinv = level_dinv<T>(L);
-  if (x_zero) {
-    ++g_klaunch;
-    k_cheb_first<T><<<tpb(nn), 256, 0, c.stream>>>(b, dinv, x, r, d, Ad, L.cheb, nn);
-  } else {
+  if (mode == 0) {
+    klaunch(k_cheb_first<T>, tpb(nn), 256, 0, c.stream, b, dinv, x, r, d, Ad, L.cheb, nn);
+  } else if (mode == 2) {
     launch_apply_K_acc<T, T>(L.g, level_K<T>(L), x, r, c.stream);
-    ++g_klaunch;
-    k_cheb_first_x<T><<<tpb(nn), 256, 0, c.stream>>>(b, dinv, x, r, d, Ad, L.cheb, nn);
+    klaunch(k_cheb_first_x<T>, tpb(nn), 256, 0, c.stream, b, dinv, x, r, d, Ad, L.cheb, nn);
   }
   for (int k = 1; k < c.mg_degree; ++k) {
     launch_apply_K_acc<T, T>(L.g, level_K<T>(L), d, Ad, c.stream);
-    ++g_klaunch;
-    k_cheb_step<T><<<tpb(nn), 256, 0, c.stream>>>(Ad, dinv, x, r, d, L.cheb + 2 * k, nn);
+    klaunch(k_cheb_step<T>, tpb(nn), 256, 0, c.stream, Ad, dinv, x, r, d, L.cheb + 2 * k, nn);
   }
   DP_LAUNCH_CHECK();
 }
 
+// first_done: the level's first pre-smoothing step was fused into the restriction.
 template <typename T>
-static void vcycle(Ctx& c, size_t l, const T* b, T* x, const MGOptions& o) {
+static void vcycle(Ctx& c, size_t l, const T* b, T* x, const MGOptions& o, bool first_done) {
   MGLevel& L = c.mg[l];
+  const bool dense_coarsest = c.coarse_n > 0;
   if (l + 1 == c.mg.size()) {
-    if (c.coarse_n > 0) {
+    if (dense_coarsest) {
       // dense inverse: identity rows on constrained DOFs keep them at zero
       const int nn = (int)c.coarse_n;
-      const double* Inv = c.coarse_chol + (size_t)nn * nn;
-      ++g_klaunch;
-      k_dense_apply<T><<<(int)div_up(nn, 8), 256, 0, c.stream>>>(Inv, b, x, nn);
+      const double* Inv = c.coarse_inv + (size_t)nn * nn;
+      klaunch(k_dense_apply<T>, nn, 128, 0, c.stream, Inv, b, x, nn);
       DP_LAUNCH_CHECK();
     } else {
-      chebyshev<T>(c, L, b, x, true);
+      chebyshev<T>(c, L, b, x, first_done ? 1 : 0);
       for (int s = 1; s < o.coarse_sweeps; ++s) {
         DP_CUDA(cudaMemsetAsync(L.r, 0, sizeof(T) * 2 * L.g.nnod, c.stream));
-        chebyshev<T>(c, L, b, x, false);
+        chebyshev<T>(c, L, b, x, 2);
       }
     }
     return;
@@ -794,22 +824,25 @@ static void vcycle(Ctx& c, size_t l, const T* b, T* x, const MGOptions& o) {
   T* t = (T*)L.t;
   T* bc = (T*)C.b;
   T* xc = (T*)C.x;
-  // pre-smoothing, then restrict the true residual r - A d_last
-  chebyshev<T>(c, L, b, x, true);
+  // pre-smoothing, then restrict the true residual r - A d_last (and take the
+  // coarse level's first smoothing step in the same pass unless it is solved densely)
+  chebyshev<T>(c, L, b, x, first_done ? 1 : 0);
   launch_apply_K_acc<T, T>(L.g, level_K<T>(L), (const T*)L.d, t, c.stream);
-  ++g_klaunch;
-  k_restrict_g<T><<<tpb(C.g.nnod), 256, 0, c.stream>>>(r, t, bc, (int)L.g.A(), (int)L.g.B(), (int)C.g.A(),
-                                                         (int)C.g.B(), C.g.pin);
+  const bool fuse = !(l + 2 == c.mg.size() && dense_coarsest);
+  const int nA0 = (int)((C.g.A() + 1) >> 1);  // coarse nodes per parity class (upper bound)
+  dim3 grid((unsigned)div_up((int64_t)nA0 * (C.g.B() >> 1), 256), 4);
+  klaunch(k_restrict_g<T>, grid, 256, 0, c.stream, (const T*)r, (const T*)t, bc, (int)L.g.A(), (int)L.g.B(),
+          (int)C.g.A(), (int)C.g.B(), C.g.pin, fuse ? 1 : 0, (const T*)level_dinv<T>(C), xc, (T*)C.r, (T*)C.d,
+          (T*)C.t, (const double*)C.cheb);
   DP_LAUNCH_CHECK();
-  vcycle<T>(c, l + 1, bc, xc, o);
-  ++g_klaunch;
-  k_prolong_add<T><<<tpb(L.g.nnod), 256, 0, c.stream>>>(xc, x, r, (int)L.g.A(), (int)L.g.B(), C.g.ncr, (int)C.g.A(),
+  vcycle<T>(c, l + 1, bc, xc, o, fuse);
+  klaunch(k_prolong_add<T>, tpb(L.g.nnod), 256, 0, c.stream, xc, x, r, (int)L.g.A(), (int)L.g.B(), C.g.ncr, (int)C.g.A(),
                                                           (int)C.g.B(), L.g.pin);
   DP_LAUNCH_CHECK();
-  chebyshev<T>(c, L, b, x, false);
+  chebyshev<T>(c, L, b, x, 2);
 }
 
-void mg_apply(Ctx& c, const double* b, double* x, const MGOptions& o) { vcycle<double>(c, 0, b, x, o); }
-void mg_apply_f(Ctx& c, const float* b, float* x, const MGOptions& o) { vcycle<float>(c, 0, b, x, o); }
+void mg_apply(Ctx& c, const double* b, double* x, const MGOptions& o) { vcycle<double>(c, 0, b, x, o, false); }
+void mg_apply_f(Ctx& c, const float* b, float* x, const MGOptions& o) { vcycle<float>(c, 0, b, x, o, false); }
 
 }  // namespace dp

@@ -12,7 +12,7 @@ struct MGOptions {
   double cheb_hi = 1.1;
   int block_jacobi = 1;     // 1: 2x2 nodal blocks (u_theta, u_r); 0: point Jacobi
   int max_levels = 16;
-  int64_t coarse_max = 1024;// largest dense coarsest system
+  int64_t coarse_max = 1536;// largest dense coarsest system
   int coarse_sweeps = 4;    // smoothing sweeps when the coarsest is not dense
   int apply_warps = 4;      // tile of the element-by-element applies (Level::warps)
   int apply_warps_t = 1;    // (Level::warps_t)

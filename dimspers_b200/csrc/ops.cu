@@ -56,6 +56,7 @@ __device__ inline int tile_element(int ncr, int wt) {
 template <typename Tm, typename Tv>
 __global__ void __launch_bounds__(256) k_apply_K(const Tm* __restrict__ K, const Tv* __restrict__ x,
                                                  Tv* __restrict__ y, int nel, int ncr, int A, int B, int wt) {
+  grid_dep_wait();
   const int e = tile_element(ncr, wt);
   if (e >= nel) return;
   typedef typename KVec<Tm>::V VT;
@@ -130,10 +131,9 @@ template void launch_apply_K<float, float>(const Level&, const float*, const flo
 // y += K x (the caller has zeroed y, typically inside the preceding vector kernel)
 template <typename Tm, typename Tv>
 void launch_apply_K_acc(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
-  ++g_klaunch;
   int blocks, threads, wt;
   apply_tile(L, blocks, threads, wt);
-  k_apply_K<Tm, Tv><<<blocks, threads, 0, s>>>(K, x, y, (int)L.nel, L.ncr, (int)L.A(), (int)L.B(), wt);
+  klaunch(k_apply_K<Tm, Tv>, blocks, threads, 0, s, K, x, y, (int)L.nel, L.ncr, (int)L.A(), (int)L.B(), wt);
   DP_LAUNCH_CHECK();
 }
 template void launch_apply_K_acc<double, double>(const Level&, const double*, const double*, double*, cudaStream_t);
@@ -172,6 +172,7 @@ __device__ inline void element_pdofs_dev(int e, int ncr, int nct, int pressure, 
 
 __global__ void k_apply_G(const double* __restrict__ G, const double* __restrict__ p, double* __restrict__ y,
                           int nel, int ncr, int nct, int A, int B, int pressure) {
+  grid_dep_wait();
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nel) return;
   int nd[6], pd[3];
@@ -188,6 +189,7 @@ __global__ void k_apply_G(const double* __restrict__ G, const double* __restrict
 
 __global__ void k_apply_GT(const double* __restrict__ G, const double* __restrict__ x, double* __restrict__ p,
                            int nel, int ncr, int nct, int A, int B, int pressure) {
+  grid_dep_wait();
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nel) return;
   int nd[6], pd[3];
@@ -209,8 +211,7 @@ __global__ void k_apply_GT(const double* __restrict__ G, const double* __restric
 void launch_apply_G(Ctx& c, const double* p, double* y) {
   const Level& L = c.fine;
   DP_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * 2 * L.nnod, c.stream));
-  ++g_klaunch;
-  k_apply_G<<<(int)div_up(L.nel, 128), 128, 0, c.stream>>>(c.Gp, p, y, (int)L.nel, L.ncr, L.nct, (int)L.A(),
+  klaunch(k_apply_G, (int)div_up(L.nel, 128), 128, 0, c.stream, c.Gp, p, y, (int)L.nel, L.ncr, L.nct, (int)L.A(),
                                                            (int)L.B(), c.mesh.pressure);
   DP_LAUNCH_CHECK();
 }
@@ -218,8 +219,7 @@ void launch_apply_G(Ctx& c, const double* p, double* y) {
 void launch_apply_GT(Ctx& c, const double* x, double* p) {
   const Level& L = c.fine;
   if (c.mesh.pressure == 0) DP_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * c.mesh.npres, c.stream));
-  ++g_klaunch;
-  k_apply_GT<<<(int)div_up(L.nel, 128), 128, 0, c.stream>>>(c.Gp, x, p, (int)L.nel, L.ncr, L.nct, (int)L.A(),
+  klaunch(k_apply_GT, (int)div_up(L.nel, 128), 128, 0, c.stream, c.Gp, x, p, (int)L.nel, L.ncr, L.nct, (int)L.A(),
                                                             (int)L.B(), c.mesh.pressure);
   DP_LAUNCH_CHECK();
 }
@@ -228,6 +228,7 @@ void launch_apply_GT(Ctx& c, const double* x, double* p) {
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_dot(const T* __restrict__ a, const T* __restrict__ b, int64_t n,
                                                      double* partial, unsigned int* counter, double* out) {
+  grid_dep_wait();
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads)
     s += (double)a[i] * (double)b[i];
@@ -238,6 +239,7 @@ __global__ void __launch_bounds__(kRedThreads) k_dot(const T* __restrict__ a, co
 
 __global__ void __launch_bounds__(kRedThreads) k_sum(const double* __restrict__ a, int64_t n, double* partial,
                                                      unsigned int* counter, double* out) {
+  grid_dep_wait();
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads)
     s += a[i];
@@ -249,24 +251,22 @@ __global__ void __launch_bounds__(kRedThreads) k_sum(const double* __restrict__ 
 static int red_blocks(int64_t n) { return red_grid(n); }
 
 void launch_dot(Ctx& c, const double* a, const double* b, int64_t n, int slot) {
-  ++g_klaunch;
-  k_dot<double><<<red_blocks(n), kRedThreads, 0, c.stream>>>(a, b, n, c.partial, c.counter, c.scal + slot);
+  klaunch(k_dot<double>, red_blocks(n), kRedThreads, 0, c.stream, a, b, n, c.partial, c.counter, c.scal + slot);
   DP_LAUNCH_CHECK();
 }
 void launch_dot_f(Ctx& c, const float* a, const float* b, int64_t n, int slot) {
-  ++g_klaunch;
-  k_dot<float><<<red_blocks(n), kRedThreads, 0, c.stream>>>(a, b, n, c.partial, c.counter, c.scal + slot);
+  klaunch(k_dot<float>, red_blocks(n), kRedThreads, 0, c.stream, a, b, n, c.partial, c.counter, c.scal + slot);
   DP_LAUNCH_CHECK();
 }
 void launch_sum(Ctx& c, const double* a, int64_t n, int slot) {
-  ++g_klaunch;
-  k_sum<<<red_blocks(n), kRedThreads, 0, c.stream>>>(a, n, c.partial, c.counter, c.scal + slot);
+  klaunch(k_sum, red_blocks(n), kRedThreads, 0, c.stream, a, n, c.partial, c.counter, c.scal + slot);
   DP_LAUNCH_CHECK();
 }
 
 // ---- permutations between reference numbering and the lattice -------------
 __global__ void k_gather_ref2lat(const int64_t* __restrict__ ref2lat, const double* __restrict__ ref,
                                  double* __restrict__ lat, int64_t nnod, int comps) {
+  grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
   const int64_t l = ref2lat[n];
@@ -274,6 +274,7 @@ __global__ void k_gather_ref2lat(const int64_t* __restrict__ ref2lat, const doub
 }
 __global__ void k_scatter_lat2ref(const int64_t* __restrict__ ref2lat, const double* __restrict__ lat,
                                   double* __restrict__ ref, int64_t nnod, int comps) {
+  grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
   const int64_t l = ref2lat[n];
@@ -281,24 +282,22 @@ __global__ void k_scatter_lat2ref(const int64_t* __restrict__ ref2lat, const dou
 }
 void launch_gather_ref2lat(Ctx& c, const double* ref, double* lat, int comps) {
   const int64_t n = c.fine.nnod;
-  ++g_klaunch;
-  k_gather_ref2lat<<<(int)div_up(n, 256), 256, 0, c.stream>>>(c.ref2lat, ref, lat, n, comps);
+  klaunch(k_gather_ref2lat, (int)div_up(n, 256), 256, 0, c.stream, c.ref2lat, ref, lat, n, comps);
   DP_LAUNCH_CHECK();
 }
 void launch_scatter_lat2ref(Ctx& c, const double* lat, double* ref, int comps) {
   const int64_t n = c.fine.nnod;
-  ++g_klaunch;
-  k_scatter_lat2ref<<<(int)div_up(n, 256), 256, 0, c.stream>>>(c.ref2lat, lat, ref, n, comps);
+  klaunch(k_scatter_lat2ref, (int)div_up(n, 256), 256, 0, c.stream, c.ref2lat, lat, ref, n, comps);
   DP_LAUNCH_CHECK();
 }
 
 __global__ void k_pc_invert(double* pc, int64_t n) {
+  grid_dep_wait();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) pc[i] = 1.0 / pc[i];
 }
 void launch_pc_invert(Ctx& c, double* pc, int64_t n) {
-  ++g_klaunch;
-  k_pc_invert<<<(int)div_up(n, 256), 256, 0, c.stream>>>(pc, n);
+  klaunch(k_pc_invert, (int)div_up(n, 256), 256, 0, c.stream, pc, n);
   DP_LAUNCH_CHECK();
 }
 

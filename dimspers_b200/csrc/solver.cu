@@ -42,6 +42,7 @@ static int nb256(int64_t n) { return (int)div_up(n, 256); }
 
 // ---- outer vector kernels -----------------------------------------------------
 __global__ void k_sub_mean(double* __restrict__ a, int64_t n, const double* __restrict__ sum) {
+  grid_dep_wait();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) a[i] -= *sum / (double)n;
 }
@@ -51,6 +52,7 @@ __global__ void __launch_bounds__(kRedThreads) k_schur_update_p(double* __restri
                                                                  double* __restrict__ rlast, const double* __restrict__ q,
                                                                  const double* __restrict__ Sq, int64_t n,
                                                                  double* scal, double* partial, unsigned int* counter) {
+  grid_dep_wait();
   const double alpha = scal[S_RD] / scal[S_QSQ];
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
@@ -67,6 +69,7 @@ __global__ void __launch_bounds__(kRedThreads) k_schur_update_p(double* __restri
 }
 
 __global__ void k_axpy_slot(double* __restrict__ U, const double* __restrict__ z, int64_t n, const double* scal) {
+  grid_dep_wait();
   const double alpha = scal[S_RD] / scal[S_QSQ];
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) U[i] += alpha * z[i];
@@ -77,6 +80,7 @@ __global__ void __launch_bounds__(kRedThreads) k_schur_center(double* __restrict
                                                                const double* __restrict__ pc, double* __restrict__ d,
                                                                int64_t n, double* scal, double* partial,
                                                                unsigned int* counter) {
+  grid_dep_wait();
   const double m = scal[S_SUMR] / (double)n;
   double s0 = 0.0, s1 = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
@@ -95,6 +99,7 @@ __global__ void __launch_bounds__(kRedThreads) k_schur_center(double* __restrict
 // Element-block mass preconditioner (discontinuous pressure): d_e = M_e^-1 r_e.
 __global__ void k_mass_blk(const double* __restrict__ r, const double* __restrict__ Minv, double* __restrict__ d,
                            int nel) {
+  grid_dep_wait();
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nel) return;
   const double r0 = r[3 * (size_t)e], r1 = r[3 * (size_t)e + 1], r2 = r[3 * (size_t)e + 2];
@@ -110,6 +115,7 @@ __global__ void __launch_bounds__(kRedThreads) k_schur_center_blk(double* __rest
                                                                    const double* __restrict__ Minv, double* __restrict__ d,
                                                                    int nel, double* scal, double* partial,
                                                                    unsigned int* counter) {
+  grid_dep_wait();
   const double m = scal[S_SUMR] / (3.0 * (double)nel);
   double s0 = 0.0, s1 = 0.0;
   for (int e = blockIdx.x * kRedThreads + threadIdx.x; e < nel; e += gridDim.x * kRedThreads) {
@@ -136,6 +142,7 @@ __global__ void __launch_bounds__(kRedThreads) k_schur_center_blk(double* __rest
 // q = d + beta q, beta = BNUM / RD; sum(q) -> S_SUMQ (for the next rm0space!)
 __global__ void __launch_bounds__(kRedThreads) k_q_update(double* __restrict__ q, const double* __restrict__ d, int64_t n,
                                                            double* scal, double* partial, unsigned int* counter) {
+  grid_dep_wait();
   const double beta = scal[S_BNUM] / scal[S_RD];
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
@@ -152,6 +159,7 @@ __global__ void __launch_bounds__(kRedThreads) k_q_update(double* __restrict__ q
 __global__ void __launch_bounds__(kRedThreads) k_q_center_rd(double* __restrict__ q, const double* __restrict__ r,
                                                               const double* __restrict__ d, int64_t n, double* scal,
                                                               double* partial, unsigned int* counter) {
+  grid_dep_wait();
   const double m = scal[S_SUMQ] / (double)n;
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
@@ -165,14 +173,17 @@ __global__ void __launch_bounds__(kRedThreads) k_q_center_rd(double* __restrict_
 
 __global__ void k_mul_into(const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out,
                            int64_t n) {
+  grid_dep_wait();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) out[i] = a[i] * b[i];
 }
 __global__ void k_neg(double* __restrict__ a, int64_t n) {
+  grid_dep_wait();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) a[i] = -a[i];
 }
 __global__ void k_add(const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out, int64_t n) {
+  grid_dep_wait();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) out[i] = a[i] + b[i];
 }
@@ -183,6 +194,7 @@ template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_pcg_update(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
                                                              const T* __restrict__ Ap, int64_t n, double* scal, int rz_slot,
                                                              double* partial, unsigned int* counter) {
+  grid_dep_wait();
   const double alpha = scal[rz_slot] / scal[S_PAP];
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
@@ -200,6 +212,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_update(T* __restrict__ x, T
 template <typename T>
 __global__ void k_pcg_dir(T* __restrict__ p, const T* __restrict__ z, int64_t n, const double* scal, int new_slot,
                           int old_slot) {
+  grid_dep_wait();
   const double beta = scal[new_slot] / scal[old_slot];
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) p[i] = (T)((double)z[i] + beta * (double)p[i]);
@@ -207,11 +220,13 @@ __global__ void k_pcg_dir(T* __restrict__ p, const T* __restrict__ z, int64_t n,
 
 
 __global__ void k_f32_to_f64(const float* __restrict__ a, double* __restrict__ b, int64_t n) {
+  grid_dep_wait();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) b[i] = (double)a[i];
 }
 __global__ void k_bj_host_mixed(const float* __restrict__ dinv, const double* __restrict__ r, double* __restrict__ z,
                                 int64_t nnod) {
+  grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
   double z0, z1;
@@ -222,15 +237,18 @@ __global__ void k_bj_host_mixed(const float* __restrict__ dinv, const double* __
 
 template <typename T>
 __global__ void k_scale_copy(const double* __restrict__ a, T* __restrict__ b, double s, int64_t n) {
+  grid_dep_wait();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) b[i] = (T)(s * a[i]);
 }
 template <typename T>
 __global__ void k_add_scaled(double* __restrict__ z, const T* __restrict__ e, double s, int64_t n) {
+  grid_dep_wait();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) z[i] += s * (double)e[i];
 }
 __global__ void k_residual(const double* __restrict__ y, double* __restrict__ Kz, int64_t n) {  // Kz <- y - Kz
+  grid_dep_wait();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) Kz[i] = y[i] - Kz[i];
 }
@@ -274,23 +292,19 @@ static int pcg(Ctx& c, const T* Kmat, const T* b, T* x, T* r, T* z, T* p, T* Ap,
         // FP64 vectors, FP32 hierarchy: unscaled conversion (host loop is a debugging path)
         float* r32 = (float*)c.work[W_F_R];
         float* z32 = (float*)c.work[W_F_Z];
-        ++g_klaunch;
-        k_scale_copy<float><<<nb256(n), 256, 0, c.stream>>>((const double*)rin, r32, 1.0, n);
+        klaunch(k_scale_copy<float>, nb256(n), 256, 0, c.stream, (const double*)rin, r32, 1.0, n);
         mg_apply_f(c, r32, z32, mgo);
-        ++g_klaunch;
-        k_f32_to_f64<<<nb256(n), 256, 0, c.stream>>>(z32, (double*)zout, n);
+        klaunch(k_f32_to_f64, nb256(n), 256, 0, c.stream, z32, (double*)zout, n);
       } else if (std::is_same<T, double>::value) {
         mg_apply(c, (const double*)rin, (double*)zout, mgo);
       } else {
         mg_apply_f(c, (const float*)rin, (float*)zout, mgo);
       }
     } else if (c.mg_prec == 1 && std::is_same<T, double>::value) {
-      ++g_klaunch;
-      k_bj_host_mixed<<<nb256(L.nnod), 256, 0, c.stream>>>(c.mg[0].dinv32, (const double*)rin, (double*)zout, L.nnod);
+      klaunch(k_bj_host_mixed, nb256(L.nnod), 256, 0, c.stream, c.mg[0].dinv32, (const double*)rin, (double*)zout, L.nnod);
     } else {
       const T* dinv = std::is_same<T, double>::value ? (const T*)c.mg[0].dinv64 : (const T*)c.mg[0].dinv32;
-      ++g_klaunch;
-      k_bj<T><<<nb256(L.nnod), 256, 0, c.stream>>>(dinv, rin, zout, L.nnod);
+      klaunch(k_bj<T>, nb256(L.nnod), 256, 0, c.stream, dinv, rin, zout, L.nnod);
     }
   };
   precond(r, z);
@@ -303,16 +317,14 @@ static int pcg(Ctx& c, const T* Kmat, const T* b, T* x, T* r, T* z, T* p, T* Ap,
     const int nxt = (it & 1) ? S_RZ1 : S_RZ0;
     launch_apply_K<T, T>(L, Kmat, p, Ap, c.stream);
     dot_t<T>(c, p, Ap, n, S_PAP);
-    ++g_klaunch;
-    k_pcg_update<T><<<red_grid(n), kRedThreads, 0, c.stream>>>(x, r, p, Ap, n, c.scal, cur, c.partial, c.counter);
+    klaunch(k_pcg_update<T>, red_grid(n), kRedThreads, 0, c.stream, x, r, p, Ap, n, c.scal, cur, c.partial, c.counter);
     DP_LAUNCH_CHECK();
     rr = read_slot(c, S_IRR);
     if (!std::isfinite(rr)) break;
     if (rr <= tol2) break;
     precond(r, z);
     dot_t<T>(c, r, z, n, nxt);
-    ++g_klaunch;
-    k_pcg_dir<T><<<nb256(n), 256, 0, c.stream>>>(p, z, n, c.scal, nxt, cur);
+    klaunch(k_pcg_dir<T>, nb256(n), 256, 0, c.stream, p, z, n, c.scal, nxt, cur);
     DP_LAUNCH_CHECK();
   }
   if (out_relres) *out_relres = std::sqrt(rr / bb);
@@ -352,16 +364,13 @@ int inner_solve(Ctx& c, const double* y, double* z, const SolveCfg& cfg, InnerSt
   int total = 0;
   for (int ref = 0; ref < cfg.max_refine; ++ref) {
     const double s = std::sqrt(rel * rel * yy);
-    ++g_klaunch;
-    k_scale_copy<float><<<nb256(n), 256, 0, c.stream>>>(res, fb, 1.0 / s, n);
+    klaunch(k_scale_copy<float>, nb256(n), 256, 0, c.stream, res, fb, 1.0 / s, n);
     double rel32 = 0.0;
     total += pcg<float>(c, c.K32, fb, fx, fr, fz, fp, fAp, cfg.inner_rtol32, cfg.inner_itmax, cfg.inner_pc, cfg.mg,
                         &rel32);
-    ++g_klaunch;
-    k_add_scaled<float><<<nb256(n), 256, 0, c.stream>>>(z, fx, s, n);
+    klaunch(k_add_scaled<float>, nb256(n), 256, 0, c.stream, z, fx, s, n);
     launch_apply_K<double, double>(L, c.K64, z, res, c.stream);
-    ++g_klaunch;
-    k_residual<<<nb256(n), 256, 0, c.stream>>>(y, res, n);
+    klaunch(k_residual, nb256(n), 256, 0, c.stream, y, res, n);
     DP_LAUNCH_CHECK();
     launch_dot(c, res, res, n, S_TMP);
     rel = std::sqrt(read_slot(c, S_TMP) / yy);
@@ -379,6 +388,7 @@ __global__ void __launch_bounds__(kRedThreads) k_rot_integrals(const double* __r
                                                                 const double* __restrict__ r_lat, int nel, int ncr, int A,
                                                                 int B, double* scal, double* partial,
                                                                 unsigned int* counter) {
+  grid_dep_wait();
   double am = 0.0, mom = 0.0;
   for (int e = blockIdx.x * kRedThreads + threadIdx.x; e < nel; e += gridDim.x * kRedThreads) {
     int nd[6];
@@ -410,6 +420,7 @@ __global__ void __launch_bounds__(kRedThreads) k_rot_integrals(const double* __r
 }
 
 __global__ void k_rot_remove(double* __restrict__ U, const double* __restrict__ r_lat, int64_t nnod, const double* scal) {
+  grid_dep_wait();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= nnod) return;
   const double om = scal[S_AM] / scal[S_MOM];
@@ -419,6 +430,7 @@ __global__ void k_rot_remove(double* __restrict__ U, const double* __restrict__ 
 // U_cart = TT U per node: [c s; -s c] (StokesSolver.jl:159, :214-241)
 __global__ void k_to_cartesian(const double* __restrict__ U, const double* __restrict__ th, double* __restrict__ Uc,
                                int64_t nnod) {
+  grid_dep_wait();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= nnod) return;
   double s, c;
@@ -445,17 +457,14 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
   // Rhs = F + G P ; U = K^-1 Rhs   (IterativeSolvers.jl:101-111)
   if (!cfg.use_guess) DP_CUDA(cudaMemsetAsync(P, 0, sizeof(double) * nP, c.stream));
   launch_apply_G(c, P, y);
-  ++g_klaunch;
-  k_add<<<nb256(nU), 256, 0, c.stream>>>(c.F, y, rhs, nU);
+  klaunch(k_add, nb256(nU), 256, 0, c.stream, c.F, y, rhs, nU);
   DP_LAUNCH_CHECK();
   inner_solve(c, rhs, U, cfg, st);
   // r = -G^T U; rm0space!(r)
   launch_apply_GT(c, U, r);
-  ++g_klaunch;
-  k_neg<<<nb256(nP), 256, 0, c.stream>>>(r, nP);
+  klaunch(k_neg, nb256(nP), 256, 0, c.stream, r, nP);
   launch_sum(c, r, nP, S_SUMR);
-  ++g_klaunch;
-  k_sub_mean<<<nb256(nP), 256, 0, c.stream>>>(r, nP, c.scal + S_SUMR);
+  klaunch(k_sub_mean, nb256(nP), 256, 0, c.stream, r, nP, c.scal + S_SUMR);
   launch_dot(c, r, r, nP, S_RR);
   DP_LAUNCH_CHECK();
   const double r0 = std::sqrt(read_slot(c, S_RR));
@@ -463,11 +472,9 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
   const double tol = r0 * cfg.rtol;
   // d = r .* pc (or M^-1 r); q = d
   if (cfg.schur_pc == 1) {
-    ++g_klaunch;
-    k_mass_blk<<<nb256(L.nel), 256, 0, c.stream>>>(r, c.Minv, d, (int)L.nel);
+    klaunch(k_mass_blk, nb256(L.nel), 256, 0, c.stream, r, c.Minv, d, (int)L.nel);
   } else {
-    ++g_klaunch;
-    k_mul_into<<<nb256(nP), 256, 0, c.stream>>>(r, c.pc, d, nP);
+    klaunch(k_mul_into, nb256(nP), 256, 0, c.stream, r, c.pc, d, nP);
   }
   DP_CUDA(cudaMemcpyAsync(q, d, sizeof(double) * nP, cudaMemcpyDeviceToDevice, c.stream));
   launch_sum(c, q, nP, S_SUMQ);
@@ -477,25 +484,21 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
   if (r0 == 0.0) res.status = 0;
   for (int it = 1; it <= cfg.itmax && r0 > 0.0; ++it) {
     // rm0space!(q); rd = r.d
-    ++g_klaunch;
-    k_q_center_rd<<<red_grid(nP), kRedThreads, 0, c.stream>>>(q, r, d, nP, c.scal, c.partial, c.counter);
+    klaunch(k_q_center_rd, red_grid(nP), kRedThreads, 0, c.stream, q, r, d, nP, c.scal, c.partial, c.counter);
     // y = G q ; z = K^-1 y ; Sq = G^T z ; qSq
     launch_apply_G(c, q, y);
     inner_solve(c, y, z, cfg, st);
     launch_apply_GT(c, z, Sq);
     launch_dot(c, q, Sq, nP, S_QSQ);
     // P += alpha q; U += alpha z; r -= alpha Sq
-    ++g_klaunch;
-    k_schur_update_p<<<red_grid(nP), kRedThreads, 0, c.stream>>>(P, r, rlast, q, Sq, nP, c.scal, c.partial, c.counter);
-    ++g_klaunch;
-    k_axpy_slot<<<nb256(nU), 256, 0, c.stream>>>(U, z, nU, c.scal);
+    klaunch(k_schur_update_p, red_grid(nP), kRedThreads, 0, c.stream, P, r, rlast, q, Sq, nP, c.scal, c.partial, c.counter);
+    klaunch(k_axpy_slot, nb256(nU), 256, 0, c.stream, U, z, nU, c.scal);
     // rm0space!(r); d = r .* pc; ||r||; (r - rlast).d
-    ++g_klaunch;
     if (cfg.schur_pc == 1)
-      k_schur_center_blk<<<red_grid(L.nel), kRedThreads, 0, c.stream>>>(r, rlast, c.Minv, d, (int)L.nel, c.scal,
+      klaunch(k_schur_center_blk, red_grid(L.nel), kRedThreads, 0, c.stream, r, rlast, c.Minv, d, (int)L.nel, c.scal,
                                                                          c.partial, c.counter);
     else
-      k_schur_center<<<red_grid(nP), kRedThreads, 0, c.stream>>>(r, rlast, c.pc, d, nP, c.scal, c.partial, c.counter);
+      klaunch(k_schur_center, red_grid(nP), kRedThreads, 0, c.stream, r, rlast, c.pc, d, nP, c.scal, c.partial, c.counter);
     DP_LAUNCH_CHECK();
     read_slots(c, 0, 6);
     const double qSq = c.h_scal[S_QSQ], rd = c.h_scal[S_RD];
@@ -513,8 +516,7 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
       break;
     }
     // q = d + beta q
-    ++g_klaunch;
-    k_q_update<<<red_grid(nP), kRedThreads, 0, c.stream>>>(q, d, nP, c.scal, c.partial, c.counter);
+    klaunch(k_q_update, red_grid(nP), kRedThreads, 0, c.stream, q, d, nP, c.scal, c.partial, c.counter);
     DP_LAUNCH_CHECK();
   }
   res.relres = r0 > 0.0 ? rnorm / r0 : 0.0;
@@ -523,10 +525,8 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
   // residual diagnostics on the raw solution: ||K U - F - G P|| / ||F||, ||G^T U||
   launch_apply_K<double, double>(L, c.K64, U, rhs, c.stream);   // rhs <- K U
   launch_apply_G(c, P, y);                                      // y <- G P
-  ++g_klaunch;
-  k_add<<<nb256(nU), 256, 0, c.stream>>>(c.F, y, y, nU);        // y <- F + G P
-  ++g_klaunch;
-  k_residual<<<nb256(nU), 256, 0, c.stream>>>(y, rhs, nU);      // rhs <- F + G P - K U
+  klaunch(k_add, nb256(nU), 256, 0, c.stream, c.F, y, y, nU);        // y <- F + G P
+  klaunch(k_residual, nb256(nU), 256, 0, c.stream, y, rhs, nU);      // rhs <- F + G P - K U
   DP_LAUNCH_CHECK();
   launch_dot(c, rhs, rhs, nU, S_TMP);
   launch_dot(c, c.F, c.F, nU, S_TMP2);
@@ -534,19 +534,16 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
   res.mom_residual = std::sqrt(c.h_scal[S_TMP] / std::max(c.h_scal[S_TMP2], 1e-300));
   launch_apply_GT(c, U, Sq);
   launch_sum(c, Sq, nP, S_SUMR);
-  ++g_klaunch;
-  k_sub_mean<<<nb256(nP), 256, 0, c.stream>>>(Sq, nP, c.scal + S_SUMR);
+  klaunch(k_sub_mean, nb256(nP), 256, 0, c.stream, Sq, nP, c.scal + S_SUMR);
   launch_dot(c, Sq, Sq, nP, S_TMP);
   res.div_residual = r0 > 0.0 ? std::sqrt(read_slot(c, S_TMP)) / r0 : 0.0;
 
   // rigid-rotation removal (updatevelocity2)
   res.omega = 0.0;
   if (cfg.remove_rotation) {
-    ++g_klaunch;
-    k_rot_integrals<<<red_grid(L.nel), kRedThreads, 0, c.stream>>>(U, c.rho_lat, c.theta_lat, c.r_lat, (int)L.nel, L.ncr,
+    klaunch(k_rot_integrals, red_grid(L.nel), kRedThreads, 0, c.stream, U, c.rho_lat, c.theta_lat, c.r_lat, (int)L.nel, L.ncr,
                                                                    (int)L.A(), (int)L.B(), c.scal, c.partial, c.counter);
-    ++g_klaunch;
-    k_rot_remove<<<nb256(L.nnod), 256, 0, c.stream>>>(U, c.r_lat, L.nnod, c.scal);
+    klaunch(k_rot_remove, nb256(L.nnod), 256, 0, c.stream, U, c.r_lat, L.nnod, c.scal);
     DP_LAUNCH_CHECK();
     read_slots(c, S_AM, 2);
     res.omega = c.h_scal[S_AM] / c.h_scal[S_MOM];
@@ -555,8 +552,7 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
 }
 
 void to_cartesian(Ctx& c, const double* U, double* Uc) {
-  ++g_klaunch;
-  k_to_cartesian<<<nb256(c.fine.nnod), 256, 0, c.stream>>>(U, c.theta_lat, Uc, c.fine.nnod);
+  klaunch(k_to_cartesian, nb256(c.fine.nnod), 256, 0, c.stream, U, c.theta_lat, Uc, c.fine.nnod);
   DP_LAUNCH_CHECK();
 }
 

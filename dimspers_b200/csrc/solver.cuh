@@ -21,7 +21,15 @@ struct SolveCfg {
   int host_loop = 0;        // 1: host-driven loops (debug); 0: one CUDA graph per solve
   double inner_relax = 0.0; // > 0: relaxed inner tolerance with this cap
   int schur_pc = 0;         // 0 lumped mass (StokesPcCG), 1 element-block mass inverse
+  int launch_overlap = 1;   // 1: programmatic dependent launch between solver kernels
   MGOptions mg;
+};
+
+// Sets g_pdl for the kernels launched in its scope (solve capture or host loop).
+struct PdlScope {
+  int saved;
+  explicit PdlScope(int on) : saved(g_pdl) { g_pdl = on; }
+  ~PdlScope() { g_pdl = saved; }
 };
 
 struct InnerStats {

@@ -97,6 +97,9 @@ typedef struct {
                               (1, 2, 4, 8; 0 = default 4)                     */
   int32_t apply_warps_t;   /* of those, warps stacked along theta (1 = linear
                               element order; 0 = default 1)                   */
+  int32_t launch_overlap;  /* 1 = each solver kernel may launch while its
+                              predecessor runs (programmatic dependent launch;
+                              default), 0 = plain stream order               */
 } dp_solve_opts;
 
 typedef struct {
