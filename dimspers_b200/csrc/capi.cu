@@ -124,6 +124,8 @@ static SolveCfg make_cfg(const dp_solve_opts* o) {
   if (cfg.schur_pc != 0 && cfg.schur_pc != 1) throw BadArg("schur_pc must be 0 (lumped) or 1 (mass)");
   if (o->launch_overlap != 0 && o->launch_overlap != 1) throw BadArg("launch_overlap must be 0 or 1");
   cfg.launch_overlap = o->launch_overlap;
+  if (o->mg_tail < 0) throw BadArg("mg_tail must be 0 (off) or a positive element count");
+  cfg.mg.tail_max_el = o->mg_tail;
   if (o->apply_warps > 0) cfg.mg.apply_warps = o->apply_warps;
   if (o->apply_warps_t > 0) cfg.mg.apply_warps_t = o->apply_warps_t;
   {
@@ -321,6 +323,7 @@ void dp_default_opts(dp_solve_opts* o) {
   o->apply_warps = 4;
   o->apply_warps_t = 1;
   o->launch_overlap = 1;
+  o->mg_tail = 0;
 }
 
 const char* dp_status_string(int s) {

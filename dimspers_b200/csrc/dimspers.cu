@@ -4,6 +4,7 @@
 #include "assemble.cu"
 #include "ops.cu"
 #include "mg.cu"
+#include "mgtail.cu"
 #include "solver.cu"
 #include "graph.cu"
 #include "capi.cu"

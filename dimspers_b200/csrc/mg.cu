@@ -801,6 +801,10 @@ static void chebyshev(Ctx& c, MGLevel& L, const T* b, T* x, int mode) {
 // first_done: the level's first pre-smoothing step was fused into the restriction.
 template <typename T>
 static void vcycle(Ctx& c, size_t l, const T* b, T* x, const MGOptions& o, bool first_done) {
+  if (l == tail_start(c, o)) {
+    launch_vcycle_tail<T>(c, l, b, x, first_done, o);
+    return;
+  }
   MGLevel& L = c.mg[l];
   const bool dense_coarsest = c.coarse_n > 0;
   if (l + 1 == c.mg.size()) {

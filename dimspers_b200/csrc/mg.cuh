@@ -14,6 +14,7 @@ struct MGOptions {
   int max_levels = 16;
   int64_t coarse_max = 1536;// largest dense coarsest system
   int coarse_sweeps = 4;    // smoothing sweeps when the coarsest is not dense
+  int64_t tail_max_el = 0;  // levels up to this many elements run as one cluster kernel (0: off)
   int apply_warps = 4;      // tile of the element-by-element applies (Level::warps)
   int apply_warps_t = 1;    // (Level::warps_t)
 };
@@ -43,5 +44,11 @@ void mg_setup(Ctx& c, int precision, const MGOptions& o);
 void mg_free(Ctx& c);
 void mg_apply(Ctx& c, const double* b, double* x, const MGOptions& o);
 void mg_apply_f(Ctx& c, const float* b, float* x, const MGOptions& o);
+
+// The small levels as one thread-block-cluster kernel (mgtail.cu): first level
+// it covers, and its launcher (V-cycle of levels l0.. with b, x of level l0).
+size_t tail_start(const Ctx& c, const MGOptions& o);
+template <typename T>
+void launch_vcycle_tail(Ctx& c, size_t l0, const T* b, T* x, bool first_done, const MGOptions& o);
 
 }  // namespace dp

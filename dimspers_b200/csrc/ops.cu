@@ -53,12 +53,11 @@ __device__ inline int tile_element(int ncr, int wt) {
   return 32 * m + 2 * ncr * it + lane;
 }
 
-template <typename Tm, typename Tv>
-__global__ void __launch_bounds__(256) k_apply_K(const Tm* __restrict__ K, const Tv* __restrict__ x,
-                                                 Tv* __restrict__ y, int nel, int ncr, int A, int B, int wt) {
-  grid_dep_wait();
-  const int e = tile_element(ncr, wt);
-  if (e >= nel) return;
+// y += K_e x_e for element e.  kL2: read x with ld.global.cg (L2 only), for
+// callers where other CTAs rewrite x during the same kernel.
+template <typename Tm, typename Tv, bool kL2>
+__device__ __forceinline__ void apply_element(const Tm* __restrict__ K, const Tv* x, Tv* y, int e, int ncr, int A,
+                                              int B) {
   typedef typename KVec<Tm>::V VT;
   constexpr int NV = KVec<Tm>::n;
   constexpr int PER = sizeof(VT) / sizeof(Tm);
@@ -87,7 +86,7 @@ __global__ void __launch_bounds__(256) k_apply_K(const Tm* __restrict__ K, const
   Tv xe[12], ye[12];
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
-    const X2 v = x2[nd[k]];
+    const X2 v = kL2 ? __ldcg(x2 + nd[k]) : x2[nd[k]];
     xe[2 * k] = v.x;
     xe[2 * k + 1] = v.y;
     ye[2 * k] = 0;
@@ -104,6 +103,15 @@ __global__ void __launch_bounds__(256) k_apply_K(const Tm* __restrict__ K, const
   }
 #pragma unroll
   for (int k = 0; k < 6; ++k) atomic_add2(&y[2 * nd[k]], ye[2 * k], ye[2 * k + 1]);
+}
+
+template <typename Tm, typename Tv>
+__global__ void __launch_bounds__(256) k_apply_K(const Tm* __restrict__ K, const Tv* __restrict__ x,
+                                                 Tv* __restrict__ y, int nel, int ncr, int A, int B, int wt) {
+  grid_dep_wait();
+  const int e = tile_element(ncr, wt);
+  if (e >= nel) return;
+  apply_element<Tm, Tv, false>(K, x, y, e, ncr, A, B);
 }
 
 // Grid of the tiled apply; the stacked tile only where it divides the lattice

@@ -100,6 +100,10 @@ typedef struct {
   int32_t launch_overlap;  /* 1 = each solver kernel may launch while its
                               predecessor runs (programmatic dependent launch;
                               default), 0 = plain stream order               */
+  int32_t mg_tail;         /* > 0: multigrid levels of at most this many
+                              elements run as one thread-block-cluster kernel
+                              (0 = off, the default: on B200 a cluster phase
+                              costs about as much as a kernel launch)        */
 } dp_solve_opts;
 
 typedef struct {

@@ -147,3 +147,17 @@ def test_autotune_records_and_replays(tmp_path):
             (table[key]["apply_warps"], table[key]["apply_warps_t"], table[key]["cheb_degree"])
         U, P, _, r = c.solve(want_cart=False, itmax=5000, **o)
         assert r["status"] == 0
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_cluster_tail_matches_separate_levels(precision):
+    """The V-cycle's small levels as one cluster kernel (mg_tail) give the
+    solve of the separate level kernels."""
+    c = _ctx(32, 128, "discontinuous", "aniso", 7)
+    with c:
+        U0, P0, _, r0 = c.solve(want_cart=False, precision=precision, schur_pc=1, **TIGHT)
+        for tail in (1024, 16384):
+            U1, P1, _, r1 = c.solve(want_cart=False, precision=precision, schur_pc=1, mg_tail=tail, **TIGHT)
+            assert r1["status"] == 0
+            assert abs(r1["iterations"] - r0["iterations"]) <= max(3, r0["iterations"] // 50)
+            assert rel(U1, U0) < 1e-7 and rel(P1, P0) < 1e-7
