@@ -695,9 +695,13 @@ int dp_profile_kernel(dp_ctx* h, int32_t which, int32_t reps, int32_t flush_l2, 
     float* y32 = (float*)c.work[W_F_AP];
     DP_CUDA(cudaMemsetAsync(x64, 0, sizeof(double) * n, c.stream));
     DP_CUDA(cudaMemsetAsync(x32, 0, sizeof(float) * n, c.stream));
+    // the applies accumulate into y (x is zero, so y stays zero): the events
+    // bracket the kernel alone, not the zeroing that launch_apply_K adds
+    DP_CUDA(cudaMemsetAsync(y64, 0, sizeof(double) * n, c.stream));
+    DP_CUDA(cudaMemsetAsync(y32, 0, sizeof(float) * n, c.stream));
     auto once = [&] {
-      if (which == 0) launch_apply_K<float, float>(c.fine, c.K32, x32, y32, c.stream);
-      else if (which == 1) launch_apply_K<double, double>(c.fine, c.K64, x64, y64, c.stream);
+      if (which == 0) launch_apply_K_acc<float, float>(c.fine, c.K32, x32, y32, c.stream);
+      else if (which == 1) launch_apply_K_acc<double, double>(c.fine, c.K64, x64, y64, c.stream);
       else if (c.mg_prec == 1) mg_apply_f(c, x32, y32, MGOptions());
       else mg_apply(c, x64, y64, MGOptions());
     };
