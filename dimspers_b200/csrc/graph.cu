@@ -63,18 +63,6 @@ __global__ void k_in_init(cudaGraphConditionalHandle h, DevCtl* ctl, const doubl
   cudaGraphSetConditional(h, (yy > 0.0 && yy > tol2) ? 1u : 0u);
 }
 
-__global__ void k_in_check(cudaGraphConditionalHandle h, DevCtl* ctl, double* scal, int rz, int rzn, int irr, int fp32) {
-  grid_dep_wait();
-  int it;
-  double tol2;
-  if (fp32) { it = ++ctl->in32_it; tol2 = ctl->in32_tol2; ctl->in32_total += 1; }
-  else { it = ++ctl->in_it; tol2 = ctl->in_tol2; ctl->in_total += 1; }
-  scal[rz] = scal[rzn];
-  const double rr = scal[irr];
-  const bool go = isfinite(rr) && rr > tol2 && it < ctl->inner_itmax;
-  cudaGraphSetConditional(h, go ? 1u : 0u);
-}
-
 __global__ void k_ref_init(cudaGraphConditionalHandle h, DevCtl* ctl, double* scal, int relax) {
   grid_dep_wait();
   const double yy = scal[R_YY];
@@ -170,13 +158,6 @@ __global__ void k_r_to_f32(const double* __restrict__ r, float* __restrict__ r32
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) r32[i] = (float)(s * r[i]);
 }
-__global__ void k_z_from_f32(const float* __restrict__ z32, double* __restrict__ z, const double* scal, int irr,
-                             int64_t n) {
-  grid_dep_wait();
-  const double s = sqrt(scal[irr]);
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < n) z[i] = s * (double)z32[i];
-}
 // nodal block Jacobi with an inverse of another precision
 template <typename Td, typename Tv>
 __global__ void k_bj_mixed(const Td* __restrict__ dinv, const Tv* __restrict__ r, Tv* __restrict__ z, int64_t nnod) {
@@ -190,10 +171,34 @@ __global__ void k_bj_mixed(const Td* __restrict__ dinv, const Tv* __restrict__ r
 }
 
 // x += alpha p; r -= alpha Ap; alpha = rzn/pAp; ||r||^2 -> irr
+
+// z = ||r|| z32 (the V-cycle ran on r / ||r||) fused with rz = r . z
+__global__ void __launch_bounds__(kRedThreads) k_z_from_f32_dot(const float* __restrict__ z32, double* __restrict__ z,
+                                                                 const double* __restrict__ r, double* scal, int irr,
+                                                                 int rzn, int64_t n, double* partial,
+                                                                 unsigned int* counter) {
+  grid_dep_wait();
+  const double sc = sqrt(scal[irr]);
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
+    const double zi = sc * (double)z32[i];
+    z[i] = zi;
+    s += r[i] * zi;
+  }
+  double v[1] = {s};
+  double* o[1] = {scal + rzn};
+  grid_finish<1>(v, partial, counter, o);
+}
+
+// x += alpha p; r -= alpha Ap; ||r||^2 (alpha = rz / pAp from the table); the
+// last block also takes the loop's stopping decision: continue while
+// ||r||^2 > tol^2 ||b||^2 and it < inner_itmax.
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_pcg_upd_g(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
-                                                            const T* __restrict__ Ap, int64_t n, double* scal, int rzn,
-                                                            int pap, int irr, double* partial, unsigned int* counter) {
+__global__ void __launch_bounds__(kRedThreads) k_pcg_upd_check(T* __restrict__ x, T* __restrict__ r,
+                                                                const T* __restrict__ p, const T* __restrict__ Ap,
+                                                                int64_t n, double* scal, int rz, int rzn, int pap,
+                                                                int irr, double* partial, unsigned int* counter,
+                                                                cudaGraphConditionalHandle h, DevCtl* ctl, int fp32) {
   grid_dep_wait();
   const double alpha = scal[rzn] / scal[pap];
   double s = 0.0;
@@ -205,7 +210,16 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_upd_g(T* __restrict__ x, T*
   }
   double v[1] = {s};
   double* o[1] = {scal + irr};
-  grid_finish<1>(v, partial, counter, o);
+  if (grid_finish<1>(v, partial, counter, o) && threadIdx.x == 0) {
+    int it;
+    double tol2;
+    if (fp32) { it = ++ctl->in32_it; tol2 = ctl->in32_tol2; ctl->in32_total += 1; }
+    else { it = ++ctl->in_it; tol2 = ctl->in_tol2; ctl->in_total += 1; }
+    scal[rz] = scal[rzn];
+    const double rr = scal[irr];
+    const bool go = isfinite(rr) && rr > tol2 && it < ctl->inner_itmax;
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+  }
 }
 
 __global__ void k_to_f32_scaled(const double* __restrict__ a, float* __restrict__ b, const double* scal, int64_t n) {
@@ -313,7 +327,6 @@ static void emit_pcg(Ctx& c, const SolveCfg& cfg, const T* Kmat, const T* b, T* 
         float* z32 = (float*)c.work[W_F_Z];
         klaunch(k_r_to_f32, g_nb(n), 256, 0, c.stream, (const double*)r, r32, c.scal, IRR, n);
         mg_apply_f(c, r32, z32, cfg.mg);
-        klaunch(k_z_from_f32, g_nb(n), 256, 0, c.stream, z32, (double*)z, c.scal, IRR, n);
       } else {
         mg_apply(c, (const double*)r, (double*)z, cfg.mg);
       }
@@ -321,15 +334,17 @@ static void emit_pcg(Ctx& c, const SolveCfg& cfg, const T* Kmat, const T* b, T* 
       if (c.mg_prec == 1) klaunch(k_bj_mixed<float, T>, g_nb(L.nnod), 256, 0, c.stream, c.mg[0].dinv32, r, z, L.nnod);
       else klaunch(k_bj_mixed<double, T>, g_nb(L.nnod), 256, 0, c.stream, c.mg[0].dinv64, r, z, L.nnod);
     }
-    if (f32) launch_dot_f(c, (const float*)r, (const float*)z, n, RZN);
+    if (cfg.inner_pc == 0 && !f32 && c.mg_prec == 1)
+      klaunch(k_z_from_f32_dot, red_grid(n), kRedThreads, 0, c.stream, (const float*)c.work[W_F_Z], (double*)z,
+              (const double*)r, c.scal, IRR, RZN, n, c.partial, c.counter);
+    else if (f32) launch_dot_f(c, (const float*)r, (const float*)z, n, RZN);
     else launch_dot(c, (const double*)r, (const double*)z, n, RZN);
     klaunch(k_pcg_dir_g<T>, g_nb(n), 256, 0, c.stream, p, z, Ap, n, c.scal, RZN, RZ, itp);
     launch_apply_K_acc<T, T>(L, Kmat, p, Ap, c.stream);
     if (f32) launch_dot_f(c, (const float*)p, (const float*)Ap, n, PAP);
     else launch_dot(c, (const double*)p, (const double*)Ap, n, PAP);
-    klaunch(k_pcg_upd_g<T>, red_grid(n), kRedThreads, 0, c.stream, x, r, p, Ap, n, c.scal, RZN, PAP, IRR, c.partial,
-                                                               c.counter);
-    klaunch(k_in_check, 1, 1, 0, c.stream, h, ctl, c.scal, RZ, RZN, IRR, f32 ? 1 : 0);
+    klaunch(k_pcg_upd_check<T>, red_grid(n), kRedThreads, 0, c.stream, x, r, p, Ap, n, c.scal, RZ, RZN, PAP, IRR,
+            c.partial, c.counter, h, ctl, f32 ? 1 : 0);
     DP_LAUNCH_CHECK();
   });
 }

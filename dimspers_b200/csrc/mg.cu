@@ -68,6 +68,7 @@ static void coarse_ref(int type, double alpha, double beta, double* xi, double* 
 // are simply absent.  This turns the restriction into a gather (no atomics,
 // no zeroing pass, deterministic).
 constexpr int kRMax = 64;
+constexpr int kRTaps = 25;  // largest stencil (vertex class)
 struct RestrictTable {
   int n[4];
   signed char da[4][kRMax], db[4][kRMax];
@@ -117,6 +118,7 @@ static void upload_restriction_table() {
           ++m;
         }
       }
+    if (m > kRTaps) throw std::runtime_error("restriction stencil larger than expected");
     R.n[cls] = m;
   }
   DP_CUDA(cudaMemcpyToSymbol(c_rtab, &R, sizeof(R)));
@@ -309,7 +311,7 @@ __global__ void k_prolong_add(const T* __restrict__ xc, T* __restrict__ xf, T* _
 // a thread keeps several gathers in flight.
 // first != 0 also takes the coarse level's first Chebyshev step from x = 0
 // (the work of k_cheb_first): rc = bc, dc = xc = coef[0] D^-1 bc, tc = 0.
-template <typename T>
+template <typename T, int LPN>
 __global__ void __launch_bounds__(256) k_restrict_g(const T* __restrict__ r, const T* __restrict__ t, T* __restrict__ bc,
                                                     int Af, int Bf, int Ac, int Bc, int pin, int first,
                                                     const T* __restrict__ dinv_c, T* __restrict__ xc, T* __restrict__ rc,
@@ -319,29 +321,41 @@ __global__ void __launch_bounds__(256) k_restrict_g(const T* __restrict__ r, con
   const int cls = blockIdx.y;
   const int pa = cls & 1, pb = cls >> 1;
   const int nA = (Ac - pa + 1) >> 1;  // coarse a = pa, pa + 2, ... <= Ac - 1
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= nA * (Bc >> 1)) return;
-  const int ac = 2 * (idx % nA) + pa, bcn = 2 * (idx / nA) + pb;
+  // LPN lanes per coarse node, each gathering every LPN-th tap (LPN = 4 on
+  // small levels: <= 7 taps per lane, all in flight; LPN = 1 on large levels,
+  // where the grid alone keeps the memory system busy), combined by shuffles
+  const int gidx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int idx = gidx / LPN, sub = gidx % LPN;
+  const bool live = idx < nA * (Bc >> 1);
+  const int ac = live ? 2 * (idx % nA) + pa : pa, bcn = live ? 2 * (idx / nA) + pb : pb;
   typedef typename V2<T>::T X2;
   const X2* r2 = reinterpret_cast<const X2*>(r);
   const X2* t2 = reinterpret_cast<const X2*>(t);
-  const int m = c_rtab.n[cls];
+  const int m = live ? c_rtab.n[cls] : 0;
   double s0 = 0.0, s1 = 0.0;
 #pragma unroll 8
-  for (int j = 0; j < m; ++j) {
-    const int a = 2 * ac + c_rtab.da[cls][j];
-    int b = 2 * bcn + c_rtab.db[cls][j];
+  for (int j = sub; j < m; j += LPN) {
+    const int jj = j;
+    const int a = 2 * ac + c_rtab.da[cls][jj];
+    int b = 2 * bcn + c_rtab.db[cls][jj];
     b += (b < 0) ? Bf : 0;
     b -= (b >= Bf) ? Bf : 0;
     const bool in = a >= 0 && a < Af;
     const int f = in ? a + Af * b : 0;
     const X2 rv = r2[f], tv = t2[f];
-    const double w = c_rtab.w[cls][j];
+    const double w = c_rtab.w[cls][jj];
     const double w0 = (in && !dof_fixed(a, b, 0, Af - 1, pin)) ? w : 0.0;
     const double w1 = (in && !dof_fixed(a, b, 1, Af - 1, pin)) ? w : 0.0;
     s0 += w0 * ((double)rv.x - (double)tv.x);
     s1 += w1 * ((double)rv.y - (double)tv.y);
   }
+  // every lane of the warp takes part in the shuffles (dead lanes add zeros)
+#pragma unroll
+  for (int o = 1; o < LPN; o <<= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+  }
+  if (!live || sub != 0) return;
   const int n = ac + Ac * bcn;
   const double b0 = dof_fixed(ac, bcn, 0, Ac - 1, pin) ? 0.0 : s0;
   const double b1 = dof_fixed(ac, bcn, 1, Ac - 1, pin) ? 0.0 : s1;
@@ -834,8 +848,9 @@ static void vcycle(Ctx& c, size_t l, const T* b, T* x, const MGOptions& o, bool 
   launch_apply_K_acc<T, T>(L.g, level_K<T>(L), (const T*)L.d, t, c.stream);
   const bool fuse = !(l + 2 == c.mg.size() && dense_coarsest);
   const int nA0 = (int)((C.g.A() + 1) >> 1);  // coarse nodes per parity class (upper bound)
-  dim3 grid((unsigned)div_up((int64_t)nA0 * (C.g.B() >> 1), 256), 4);
-  klaunch(k_restrict_g<T>, grid, 256, 0, c.stream, (const T*)r, (const T*)t, bc, (int)L.g.A(), (int)L.g.B(),
+  const bool small = C.g.nnod < 32768;
+  dim3 grid((unsigned)div_up((small ? 4 : 1) * (int64_t)nA0 * (C.g.B() >> 1), 256), 4);
+  klaunch(small ? k_restrict_g<T, 4> : k_restrict_g<T, 1>, grid, 256, 0, c.stream, (const T*)r, (const T*)t, bc, (int)L.g.A(), (int)L.g.B(),
           (int)C.g.A(), (int)C.g.B(), C.g.pin, fuse ? 1 : 0, (const T*)level_dinv<T>(C), xc, (T*)C.r, (T*)C.d,
           (T*)C.t, (const double*)C.cheb);
   DP_LAUNCH_CHECK();

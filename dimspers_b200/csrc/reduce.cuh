@@ -40,7 +40,7 @@ __device__ inline void block_sum_n(double (&v)[NV], double (*sh)[32]) {
 
 // partial: NV * gridDim.x doubles; out[j] receives the total of value j.
 template <int NV>
-__device__ inline void grid_finish(double (&v)[NV], double* partial, unsigned int* counter, double* const* out) {
+__device__ inline bool grid_finish(double (&v)[NV], double* partial, unsigned int* counter, double* const* out) {
   __shared__ double sh[NV][32];
   __shared__ bool last;
   block_sum_n<NV>(v, sh);
@@ -52,7 +52,7 @@ __device__ inline void grid_finish(double (&v)[NV], double* partial, unsigned in
     last = (ticket == gridDim.x - 1);
   }
   __syncthreads();
-  if (!last) return;
+  if (!last) return false;
   __threadfence();
   double s[NV];
 #pragma unroll
@@ -67,6 +67,7 @@ __device__ inline void grid_finish(double (&v)[NV], double* partial, unsigned in
     for (int j = 0; j < NV; ++j) *out[j] = s[j];
     *counter = 0;
   }
+  return true;  // in every thread of the last block (thread 0 holds the sums)
 }
 
 inline int red_grid(long long n) {
