@@ -83,6 +83,22 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(ms, device, world):
+    """The job's time: the largest per-rank time (one all-reduce, MAX)."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_value(units_per_rank, world, ms):
+    """Whole-job throughput: units of all ranks over the max-over-ranks time."""
+    return world * units_per_rank / (ms / 1e3)
+
+
 # ---------------------------------------------------------------- clocks ----
 REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
            0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
@@ -260,24 +276,19 @@ def run_ours(args, rank, world, local):
                 reps.append(step(precision))
             e1.record(stream)
             barrier()
-        ms = e0.elapsed_time(e1)
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(e0.elapsed_time(e1), dev, world)
         return ms, reps
 
     sampler = ClockSampler(local) if not args.no_clocks else None
     ms32, reps32 = timed(1, args.warmup, args.steps, sampler)
-    value = world * args.steps / (ms32 / 1e3)
+    value = aggregate_value(args.steps, world, ms32)
     ms_per_step = ms32 / args.steps
     U32, P32 = U_d.clone(), P_d.clone()   # the fast path's solution, for its error against FP64
 
     fp64 = None
     if not args.no_fp64:
         ms64, reps64 = timed(0, args.fp64_warmup, args.fp64_steps)
-        fp64 = {"value": world * args.fp64_steps / (ms64 / 1e3), "ms_per_step": ms64 / args.fp64_steps,
+        fp64 = {"value": aggregate_value(args.fp64_steps, world, ms64), "ms_per_step": ms64 / args.fp64_steps,
                 "outer_iterations": reps64[-1]["iterations"], "inner_iterations": reps64[-1]["inner_iterations"],
                 "status": reps64[-1]["status"], "relres": reps64[-1]["relres"],
                 "mom_residual": reps64[-1]["mom_residual"]}
@@ -318,12 +329,7 @@ def run_ours(args, rank, world, local):
             e2e_step()
         e1.record(stream)
         barrier()
-        ms_e2e = e0.elapsed_time(e1)
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([ms_e2e], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_e2e = float(t.item())
+        ms_e2e = max_over_ranks(e0.elapsed_time(e1), dev, world)
     h2d = (eta_h.numel() + dl_h.numel() + dx_h.numel() + dy_h.numel() + rho_h.numel()) * 8
     d2h = (U_h.numel() + P_h.numel()) * 8
 
@@ -368,7 +374,7 @@ def run_ours(args, rank, world, local):
         "guess_fallback": last["fallback_used"], "r0_guess_over_r0": (last["r0_guess"] / last["r0"]) if guess else None,
         "mom_residual": last["mom_residual"], "mg_levels": last["mg_levels"],
         "fp64": fp64, "fast_vs_fp64": (value / fp64["value"]) if fp64 else None, "fast_vs_fp64_error": err,
-        "e2e": ({"value": world * args.steps / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+        "e2e": ({"value": aggregate_value(args.steps, world, ms_e2e), "unit": UNIT, "h2d_bytes_per_step": h2d,
                  "d2h_bytes_per_step": d2h} if ms_e2e is not None else None),
         "gpu_launches": int(sum(r["kernel_launches"] for r in reps32)),
         "roofline": roofline, "clocks": clocks,

@@ -166,20 +166,33 @@ __device__ __forceinline__ void grid_dep_wait() {
 }
 
 inline thread_local int g_pdl = 0;
+// Scheduling priority given to kernels while a batch is captured (per-node
+// priorities of the batch graph); kNoPriority = the stream's own.
+constexpr int kNoPriority = 1 << 30;
+inline thread_local int g_prio = kNoPriority;
 
 template <typename... P, typename... A>
 inline void klaunch(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A... args) {
   ++g_klaunch;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchAttribute attr[2];
+  unsigned n = 0;
+  if (g_pdl) {
+    attr[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[n].val.programmaticStreamSerializationAllowed = 1;
+    ++n;
+  }
+  if (g_prio != kNoPriority) {
+    attr[n].id = cudaLaunchAttributePriority;
+    attr[n].val.priority = g_prio;
+    ++n;
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cfg.attrs = attr;
-  cfg.numAttrs = g_pdl ? 1u : 0u;
+  cfg.numAttrs = n;
   DP_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<P>(args)...));
 }
 

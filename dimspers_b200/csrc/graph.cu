@@ -14,6 +14,7 @@
 // baked into it (precision, preconditioner, guess, rotation removal), so the
 // instantiated graph is cached in the context and reused across assemblies;
 // tolerances and iteration caps are read from device memory at run time.
+#include <algorithm>
 #include <cstring>
 #include <stdexcept>
 
@@ -579,6 +580,7 @@ struct Batch {
   std::vector<Ctx*> ctx;
   std::vector<SolveCfg> cfg;
   std::vector<int64_t> gen;   // each context's allocation generation at capture
+  int priorities = 1;          // kernel priorities by problem size
   cudaStream_t s = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -617,25 +619,40 @@ void batch_build(Batch& b) {
     ensure_ctl(*c);
     b.gen.push_back(c->alloc_gen);
   }
+  // kernel priorities: the smaller a problem, the higher its priority, so the
+  // small solves finish early and the large ones fill the remaining SMs
+  int least = 0, greatest = 0;
+  DP_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  std::vector<int64_t> sizes;
+  for (Ctx* c : b.ctx) sizes.push_back(c->fine.nel);
+  std::vector<int64_t> distinct = sizes;
+  std::sort(distinct.begin(), distinct.end());
+  distinct.erase(std::unique(distinct.begin(), distinct.end()), distinct.end());
+  const int levels = least - greatest;  // number of priority steps (greatest is numerically lowest)
   DP_CUDA(cudaStreamBeginCapture(b.s, cudaStreamCaptureModeRelaxed));
   try {
     DP_CUDA(cudaEventRecord(b.fork, b.s));
     for (size_t i = 0; i < b.ctx.size(); ++i) {
       Ctx& c = *b.ctx[i];
       DP_CUDA(cudaStreamWaitEvent(c.stream, b.fork, 0));
+      const int rank = (int)(std::lower_bound(distinct.begin(), distinct.end(), sizes[i]) - distinct.begin());
+      const int steps = (int)distinct.size() > 1 ? (int)distinct.size() - 1 : 1;
+      g_prio = b.priorities ? greatest + (levels * rank) / steps : kNoPriority;
       capture_solve(c, b.cfg[i], (double*)c.work[W_U], (double*)c.work[W_P]);
+      g_prio = kNoPriority;
       DP_CUDA(cudaEventRecordWithFlags(b.done[i], c.stream, cudaEventRecordExternal));
       DP_CUDA(cudaEventRecord(b.join[i], c.stream));
       DP_CUDA(cudaStreamWaitEvent(b.s, b.join[i], 0));
     }
   } catch (...) {
+    g_prio = kNoPriority;
     cudaGraph_t g = nullptr;
     cudaStreamEndCapture(b.s, &g);
     if (g) cudaGraphDestroy(g);
     throw;
   }
   DP_CUDA(cudaStreamEndCapture(b.s, &b.graph));
-  DP_CUDA(cudaGraphInstantiate(&b.exec, b.graph, 0));
+  DP_CUDA(cudaGraphInstantiate(&b.exec, b.graph, b.priorities ? cudaGraphInstantiateFlagUseNodePriority : 0));
   DP_CUDA(cudaGraphUpload(b.exec, b.s));
 }
 

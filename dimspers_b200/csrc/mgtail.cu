@@ -354,19 +354,29 @@ void launch_vcycle_tail(Ctx& c, size_t l0, const T* b, T* x, bool first_done, co
   a.L[0].b = const_cast<T*>(b);
   a.L[0].x = x;
   const int cs = tail_cluster_size<T>();
-  cudaLaunchAttribute attr[2];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = (unsigned)cs;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[1].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchAttribute attr[3];
+  unsigned na = 0;
+  attr[na].id = cudaLaunchAttributeClusterDimension;
+  attr[na].val.clusterDim.x = (unsigned)cs;
+  attr[na].val.clusterDim.y = 1;
+  attr[na].val.clusterDim.z = 1;
+  ++na;
+  if (g_pdl) {
+    attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[na].val.programmaticStreamSerializationAllowed = 1;
+    ++na;
+  }
+  if (g_prio != kNoPriority) {
+    attr[na].id = cudaLaunchAttributePriority;
+    attr[na].val.priority = g_prio;
+    ++na;
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)cs);
   cfg.blockDim = dim3(kTailThreads);
   cfg.stream = c.stream;
   cfg.attrs = attr;
-  cfg.numAttrs = g_pdl ? 2u : 1u;
+  cfg.numAttrs = na;
   ++g_klaunch;
   DP_CUDA(cudaLaunchKernelEx(&cfg, k_vcycle_tail<T>, a));
 }
