@@ -32,7 +32,8 @@ class SolveOpts(C.Structure):
                 ("cheb_lo", C.c_double), ("cheb_hi", C.c_double), ("inner_relax", C.c_double),
                 ("coarse_max", C.c_int32), ("schur_pc", C.c_int32),
                 ("apply_warps", C.c_int32), ("apply_warps_t", C.c_int32),
-                ("launch_overlap", C.c_int32), ("mg_tail", C.c_int32)]
+                ("launch_overlap", C.c_int32), ("mg_tail", C.c_int32),
+                ("matrix_free", C.c_int32)]
 
 
 class SolveReport(C.Structure):

@@ -91,6 +91,7 @@ struct AsmArgs {
   double* F;           // 2*nnod, accumulated with atomics (zeroed by caller)
   double* pcsum;       // npres: disc -> 1/rowsum written; cont -> rowsum accumulated
   double* Minv;        // 6*nel: inverse of the element mass block (discontinuous pressure)
+  double* mfD;         // 36*nel or null: omega * Q^T D Q per IP, ring-major (matrix-free apply)
   CartOut cart;
 };
 
@@ -153,6 +154,17 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs p) {
   double Cel[6];
   if (p.mat_kind == MAT_TI) ti_tensor(p.C[e], p.C[p.nel + e], p.C[2 * p.nel + e], Cel);
 
+  // matrix-free form: the element is its ring's reference element (it = 0)
+  // rotated by phi = theta(v0) - theta(v0 of the reference); its polar operator
+  // is sum_ip om B0^T (Q^T D Q) B0 with Q the engineering-strain rotation by phi
+  double qc = 1.0, qs = 0.0;
+  const int ering = 2 * ir + t;                   // ring-major index of the element
+  const size_t emf = (size_t)ering * p.nct + it;
+  if (p.mfD) {
+    const int bref = (t == 0) ? 0 : 2;            // vertex 0 of the reference element
+    sincos(th[0] - p.theta_lat[2 * ir + p.A * bref], &qs, &qc);
+  }
+
   for (int ip = 0; ip < 6; ++ip) {
     const double th_ip = th[0] * c_N3[ip][0] + th[1] * c_N3[ip][1] + th[2] * c_N3[ip][2];
     const double r_ip = rr[0] * c_N3[ip][0] + rr[1] * c_N3[ip][1] + rr[2] * c_N3[ip][2];
@@ -191,6 +203,26 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs p) {
       }
       d11 = cc[0] * visc; d22 = cc[1] * visc; d33 = cc[2] * visc;
       d12 = cc[3] * visc; d13 = cc[4] * visc; d23 = cc[5] * visc;
+    }
+    if (p.mfD) {
+      // om * Q^T D Q, Q = [c^2 s^2 cs; s^2 c^2 -cs; -2cs 2cs c^2-s^2]
+      const double cc2 = qc * qc, ss2 = qs * qs, cs = qc * qs;
+      const double Q[3][3] = {{cc2, ss2, cs}, {ss2, cc2, -cs}, {-2.0 * cs, 2.0 * cs, cc2 - ss2}};
+      const double Dm[3][3] = {{d11, d12, d13}, {d12, d22, d23}, {d13, d23, d33}};
+      double M[3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) M[i][j] = Dm[i][0] * Q[0][j] + Dm[i][1] * Q[1][j] + Dm[i][2] * Q[2][j];
+      double R[3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) R[i][j] = Q[0][i] * M[0][j] + Q[1][i] * M[1][j] + Q[2][i] * M[2][j];
+      const size_t st = (size_t)p.nel;
+      double* o = p.mfD + (size_t)(ip * 6) * st + emf;
+      o[0 * st] = om * R[0][0];
+      o[1 * st] = om * R[0][1];
+      o[2 * st] = om * R[0][2];
+      o[3 * st] = om * R[1][1];
+      o[4 * st] = om * R[1][2];
+      o[5 * st] = om * R[2][2];
     }
     // omega * D * B columns: DBx_i = D (dx_i, 0, dz_i), DBz_i = D (0, dz_i, dx_i)
     double bx0[6], bx1[6], bx2[6], bz0[6], bz1[6], bz2[6];
@@ -326,6 +358,62 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs p) {
 #undef ACC
 }
 
+// Per ring (ir, t) of the matrix-free apply: the reference element's (it = 0)
+// Cartesian shape-function derivatives at the 6 IPs and its node rotations:
+// tab[ring * 84 + ip * 12 + k] = dN_k/dx, [.. + 6 + k] = dN_k/dz, [ring * 84 +
+// 72 + 2k] = cos theta_k, [.. + 1] = sin theta_k.  Same formulas as k_assemble.
+__global__ void k_mf_table(int ncr, int A, const double* __restrict__ theta_lat, const double* __restrict__ r_lat,
+                           double* __restrict__ tab) {
+  const int ring = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ring >= 2 * ncr) return;
+  const int ir = ring >> 1, t = ring & 1;
+  const int a0 = 2 * ir, b0 = 0;
+  int na[6], nb[6];
+  if (t == 0) {
+    const int aa[6] = {a0, a0, a0 + 2, a0, a0 + 1, a0 + 1};
+    const int bb[6] = {b0, b0 + 2, b0, b0 + 1, b0 + 1, b0};
+    for (int k = 0; k < 6; ++k) { na[k] = aa[k]; nb[k] = bb[k]; }
+  } else {
+    const int aa[6] = {a0, a0 + 2, a0 + 2, a0 + 1, a0 + 2, a0 + 1};
+    const int bb[6] = {b0 + 2, b0 + 2, b0, b0 + 2, b0 + 1, b0 + 1};
+    for (int k = 0; k < 6; ++k) { na[k] = aa[k]; nb[k] = bb[k]; }
+  }
+  int nd[6];
+  for (int k = 0; k < 6; ++k) nd[k] = na[k] + A * nb[k];
+  double th[3], rr[3];
+  for (int k = 0; k < 3; ++k) {
+    th[k] = theta_lat[nd[k]];
+    rr[k] = r_lat[nd[k]];
+  }
+  const double Jt0 = -th[0] + th[1], Jt1 = -th[0] + th[2];
+  const double Jr0 = -rr[0] + rr[1], Jr1 = -rr[0] + rr[2];
+  const double detJ = Jt0 * Jr1 - Jt1 * Jr0;
+  const double R31 = rr[2] - rr[0], R21 = rr[1] - rr[0];
+  const double T31 = th[2] - th[0], T21 = th[1] - th[0];
+  double* o = tab + (size_t)ring * kMfTab;
+  for (int ip = 0; ip < 6; ++ip) {
+    const double th_ip = th[0] * c_N3[ip][0] + th[1] * c_N3[ip][1] + th[2] * c_N3[ip][2];
+    const double r_ip = rr[0] * c_N3[ip][0] + rr[1] * c_N3[ip][1] + rr[2] * c_N3[ip][2];
+    double s, c;
+    sincos(th_ip, &s, &c);
+    const double inv = 1.0 / r_ip / detJ;
+    const double ix0 = (R31 * c - T31 * s * r_ip) * inv;
+    const double ix1 = (-R21 * c + T21 * s * r_ip) * inv;
+    const double iz0 = (-R31 * s - T31 * c * r_ip) * inv;
+    const double iz1 = (R21 * s + T21 * c * r_ip) * inv;
+    for (int k = 0; k < 6; ++k) {
+      o[ip * 12 + k] = ix0 * c_dN[ip][0][k] + ix1 * c_dN[ip][1][k];
+      o[ip * 12 + 6 + k] = iz0 * c_dN[ip][0][k] + iz1 * c_dN[ip][1][k];
+    }
+  }
+  for (int k = 0; k < 6; ++k) {
+    double s, c;
+    sincos(theta_lat[nd[k]], &s, &c);
+    o[72 + 2 * k] = c;
+    o[72 + 2 * k + 1] = s;
+  }
+}
+
 void launch_assemble(Ctx& c, int precision, const CartOut* cart) {
   const Level& L = c.fine;
   AsmArgs a{};
@@ -338,6 +426,7 @@ void launch_assemble(Ctx& c, int precision, const CartOut* cart) {
   a.K64 = c.K64;
   a.K32 = precision >= 1 ? c.K32 : nullptr;
   a.Gp = c.Gp; a.F = c.F; a.pcsum = c.pc; a.Minv = c.Minv;
+  a.mfD = c.mfD64;
   if (cart) a.cart = *cart;
   const size_t smem = sizeof(double) * kAcc * kAsmThreads;
   static bool attr_set = false;
@@ -351,6 +440,11 @@ void launch_assemble(Ctx& c, int precision, const CartOut* cart) {
   ++g_klaunch;
   k_assemble<<<grid, kAsmThreads, smem, c.stream>>>(a);
   DP_LAUNCH_CHECK();
+  if (c.mfT64) {
+    ++g_klaunch;
+    k_mf_table<<<(int)div_up(2 * L.ncr, 64), 64, 0, c.stream>>>(L.ncr, (int)L.A(), c.theta_lat, c.r_lat, c.mfT64);
+    DP_LAUNCH_CHECK();
+  }
   if (c.mesh.pressure == 0) launch_pc_invert(c, c.pc, c.mesh.npres);
 }
 

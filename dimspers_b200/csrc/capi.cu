@@ -29,6 +29,7 @@ Ctx::~Ctx() {
   mg_free(*this);
   cudaFree(theta_lat); cudaFree(r_lat); cudaFree(ref2lat);
   cudaFree(eta); cudaFree(C); cudaFree(rho_lat); cudaFree(rho_ref);
+  cudaFree(mfD64); cudaFree(mfT64); cudaFree(mfD32); cudaFree(mfT32);
   cudaFree(K64); cudaFree(K32); cudaFree(Gp); cudaFree(F); cudaFree(pc); cudaFree(Minv); cudaFree(Fscale);
   cudaFree(flush);
   cudaFree(scal); cudaFreeHost(h_scal); cudaFree(partial); cudaFree(counter);
@@ -124,6 +125,8 @@ static SolveCfg make_cfg(const dp_solve_opts* o) {
   if (cfg.schur_pc != 0 && cfg.schur_pc != 1) throw BadArg("schur_pc must be 0 (lumped) or 1 (mass)");
   if (o->launch_overlap != 0 && o->launch_overlap != 1) throw BadArg("launch_overlap must be 0 or 1");
   cfg.launch_overlap = o->launch_overlap;
+  if (o->matrix_free != 0 && o->matrix_free != 1) throw BadArg("matrix_free must be 0 or 1");
+  cfg.matrix_free = o->matrix_free;
   if (o->mg_tail < 0) throw BadArg("mg_tail must be 0 (off) or a positive element count");
   cfg.mg.tail_max_el = o->mg_tail;
   if (o->apply_warps > 0) cfg.mg.apply_warps = o->apply_warps;
@@ -171,13 +174,47 @@ static void ensure_k32(Ctx& c, const SolveCfg& cfg) {
   }
 }
 
+__global__ void k_f64_to_f32_plain(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+
+// Tile and matrix-free form of the fine-level applies.  The matrix-free data
+// are written by every assembly in FP64; the FP32 levels get a rounded copy.
+static void set_fine_apply(Ctx& c, const SolveCfg& cfg) {
+  c.fine.warps = cfg.mg.apply_warps;
+  c.fine.warps_t = cfg.mg.apply_warps_t;
+  c.fine.mfD64 = c.fine.mfT64 = nullptr;
+  c.fine.mfD32 = c.fine.mfT32 = nullptr;
+  if (!cfg.matrix_free || !c.mfD64) return;
+  c.fine.mfD64 = c.mfD64;
+  c.fine.mfT64 = c.mfT64;
+  if (cfg.precision >= 1) {
+    const int64_t nd = 36 * c.fine.nel, nt = (int64_t)kMfTab * 2 * c.fine.ncr;
+    if (!c.mfD32) {
+      dalloc(&c.mfD32, nd);
+      dalloc(&c.mfT32, nt);
+      c.mf32_stale = true;
+    }
+    if (c.mf32_stale) {
+      ++g_klaunch;
+      k_f64_to_f32_plain<<<(int)div_up(nd, 256), 256, 0, c.stream>>>(c.mfD64, c.mfD32, nd);
+      ++g_klaunch;
+      k_f64_to_f32_plain<<<(int)div_up(nt, 256), 256, 0, c.stream>>>(c.mfT64, c.mfT32, nt);
+      DP_LAUNCH_CHECK();
+      c.mf32_stale = false;
+    }
+    c.fine.mfD32 = c.mfD32;
+    c.fine.mfT32 = c.mfT32;
+  }
+}
+
 // Checks, the FP32 operator when needed, then the multigrid values (Galerkin
 // operators, smoother bounds, coarse inverse) of the current assembly.
 static void prepare_solve(Ctx& c, const SolveCfg& cfg) {
   check_solve_cfg(c, cfg);
-  c.fine.warps = cfg.mg.apply_warps;
-  c.fine.warps_t = cfg.mg.apply_warps_t;
   ensure_k32(c, cfg);
+  set_fine_apply(c, cfg);
   mg_setup(c, cfg.precision >= 1 ? 1 : 0, cfg.mg);
 }
 
@@ -324,6 +361,7 @@ void dp_default_opts(dp_solve_opts* o) {
   o->apply_warps_t = 1;
   o->launch_overlap = 1;
   o->mg_tail = 0;
+  o->matrix_free = 1;
 }
 
 const char* dp_status_string(int s) {
@@ -555,7 +593,12 @@ int dp_assemble(dp_ctx* h, int32_t precision) {
       dalloc(&c.K32, kstore<float>(c.fine.nel));
       DP_CUDA(cudaMemset(c.K32, 0, sizeof(float) * kstore<float>(c.fine.nel)));
     }
+    if (!c.mfD64) {
+      dalloc(&c.mfD64, 36 * c.fine.nel);
+      dalloc(&c.mfT64, (int64_t)kMfTab * 2 * c.fine.ncr);
+    }
     launch_assemble(c, precision, nullptr);
+    c.mf32_stale = true;
     c.assembled = precision;
     c.mg_prec = c.mg.empty() ? -1 : c.mg_prec;  // hierarchy values are rebuilt on the next solve
     DP_CUDA(cudaStreamSynchronize(c.stream));
@@ -596,10 +639,9 @@ int dp_solve(dp_ctx* h, double* U, double* P, double* Ucart, const dp_solve_opts
     if (!U || !P) throw BadArg("null U or P");
     SolveCfg cfg = make_cfg(opts);
     check_solve_cfg(c, cfg);
-    c.fine.warps = cfg.mg.apply_warps;
-    c.fine.warps_t = cfg.mg.apply_warps_t;
     const int64_t nn = c.fine.nnod, np = c.mesh.npres;
     ensure_k32(c, cfg);
+    set_fine_apply(c, cfg);
     cudaEvent_t e0, e1, e2;
     DP_CUDA(cudaEventCreate(&e0));
     DP_CUDA(cudaEventCreate(&e1));

@@ -31,6 +31,7 @@ constexpr int kKe = 78;   // packed lower 12x12
 constexpr int kGe = 36;   // 12x3 column-major
 constexpr int kMe = 6;    // packed lower 3x3
 constexpr int kFe = 12;
+constexpr int kMfTab = 84;  // per ring of the matrix-free apply: 6 IPs x (6 dN/dx, 6 dN/dz), 6 x (cos, sin)
 
 enum MatKind { MAT_NONE = 0, MAT_ISO = 1, MAT_FULL = 2, MAT_TI = 3 };
 
@@ -43,6 +44,13 @@ struct Level {
   // them stacked along theta (each warp = 16 radial cells x 2 triangles); the
   // stacked form needs ncr % 16 == 0 and falls back to the linear element order.
   int warps = 4, warps_t = 1;
+  // Matrix-free element apply (fine level only): om * Q^T D Q per element and
+  // IP (36 per element, ring-major) and the per-ring reference tables.  Null:
+  // the applies read the packed element matrices.
+  const double* mfD64 = nullptr;
+  const double* mfT64 = nullptr;
+  const float* mfD32 = nullptr;
+  const float* mfT32 = nullptr;
   int64_t A() const { return 2 * (int64_t)ncr + 1; }
   int64_t B() const { return 2 * (int64_t)nct; }
 };
@@ -93,6 +101,11 @@ struct Ctx {
   int assembled = -1;           // precision of the last assembly, -1 = none
   double* K64 = nullptr;        // 78*nel
   float* K32 = nullptr;         // 78*nel (refined path)
+  double* mfD64 = nullptr;      // 36*nel: matrix-free apply data (written by every assembly)
+  double* mfT64 = nullptr;      // kMfTab*2*ncr
+  float* mfD32 = nullptr;       // FP32 copies for the FP32 levels
+  float* mfT32 = nullptr;
+  bool mf32_stale = true;       // the FP32 copies predate the last assembly
   double* Gp = nullptr;         // 36*nel
   double* F = nullptr;          // 2*nnod
   double* pc = nullptr;         // npres (1/rowsum M)

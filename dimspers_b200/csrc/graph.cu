@@ -476,7 +476,8 @@ static int64_t graph_key(const SolveCfg& cfg, const Ctx& c) {
          ((int64_t)(cfg.inner_relax > 0.0) << 15) | ((int64_t)c.mg_prec << 16) | ((int64_t)cfg.schur_pc << 18) |
          ((int64_t)cfg.mg.block_jacobi << 20) | ((int64_t)(c.coarse_n > 0) << 21) |
          ((int64_t)cfg.mg.apply_warps << 24) | ((int64_t)cfg.mg.apply_warps_t << 28) |
-         ((int64_t)cfg.launch_overlap << 32) | ((int64_t)tail_start(c, cfg.mg) << 33);
+         ((int64_t)cfg.launch_overlap << 32) | ((int64_t)tail_start(c, cfg.mg) << 33) |
+         ((int64_t)cfg.matrix_free << 37);
 }
 
 void graph_free(Ctx& c) {

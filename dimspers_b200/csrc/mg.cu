@@ -425,12 +425,6 @@ __global__ void k_cheb_step(T* __restrict__ Ad, const T* __restrict__ dinv, T* _
   d[2 * n] = (T)d0; d[2 * n + 1] = (T)d1;
   x[2 * n] += (T)d0; x[2 * n + 1] += (T)d1;
 }
-template <typename T>
-__global__ void k_sub(const T* __restrict__ b, T* __restrict__ r, int64_t n) {  // r = b - r
-  grid_dep_wait();
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < n) r[i] = b[i] - r[i];
-}
 // z = D^-1 r (nodal blocks)
 template <typename T>
 __global__ void k_bj(const T* __restrict__ dinv, const T* __restrict__ r, T* __restrict__ z, int64_t nnod) {
@@ -719,7 +713,14 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
   for (MGLevel& L : c.mg) {
     L.g.warps = o.apply_warps;
     L.g.warps_t = o.apply_warps_t;
+    L.g.mfD64 = L.g.mfT64 = nullptr;
+    L.g.mfD32 = L.g.mfT32 = nullptr;
   }
+  // the fine level applies matrix-free when the fine context level does
+  c.mg[0].g.mfD64 = c.fine.mfD64;
+  c.mg[0].g.mfT64 = c.fine.mfT64;
+  c.mg[0].g.mfD32 = c.fine.mfD32;
+  c.mg[0].g.mfT32 = c.fine.mfT32;
   // Galerkin coarse operators
   for (size_t l = 1; l < c.mg.size(); ++l) {
     MGLevel& Lf = c.mg[l - 1];

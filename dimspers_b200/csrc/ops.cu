@@ -114,6 +114,106 @@ __global__ void __launch_bounds__(256) k_apply_K(const Tm* __restrict__ K, const
   apply_element<Tm, Tv, false>(K, x, y, e, ncr, A, B);
 }
 
+// ---- matrix-free element-by-element K apply (fine level) -------------------------
+// K_e (polar DOFs, constrained rows/columns masked) = sum_ip B0^T Dw_ip B0, with
+// B0 = B_cart(ref) T(ref) of the ring's reference element (it = 0) and Dw_ip =
+// om Q^T D Q the element's viscous tensor rotated into that reference frame
+// (written by the assembly).  Per element the apply reads 36 Dw values (144 B
+// in FP32 instead of 312 B of packed matrix) and does ~400 FMA: node DOFs to
+// the reference Cartesian frame, strain (exx, ezz, gxz) per IP, stress = Dw
+// strain, back-projection, back to polar.  Threads run along theta (ring-
+// major element order), so a warp shares its ring: the table reads are warp-
+// uniform and the Dw reads are coalesced.
+template <typename T>
+__global__ void __launch_bounds__(256) k_apply_K_mf(const T* __restrict__ Dw, const T* __restrict__ tab,
+                                                    const T* __restrict__ x, T* __restrict__ y, int ncr, int nct,
+                                                    int A, int B, int pin) {
+  grid_dep_wait();
+  const int nel = 2 * ncr * nct;
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= nel) return;
+  const int it = gid % nct, ring = gid / nct;
+  const int ir = ring >> 1, t = ring & 1;
+  const int a0 = 2 * ir, b0 = 2 * it;
+  int aa[6], bb[6];
+  if (t == 0) {
+    aa[0] = a0; aa[1] = a0; aa[2] = a0 + 2; aa[3] = a0; aa[4] = a0 + 1; aa[5] = a0 + 1;
+    bb[0] = b0; bb[1] = b0 + 2; bb[2] = b0; bb[3] = b0 + 1; bb[4] = b0 + 1; bb[5] = b0;
+  } else {
+    aa[0] = a0; aa[1] = a0 + 2; aa[2] = a0 + 2; aa[3] = a0 + 1; aa[4] = a0 + 2; aa[5] = a0 + 1;
+    bb[0] = b0 + 2; bb[1] = b0 + 2; bb[2] = b0; bb[3] = b0 + 2; bb[4] = b0 + 1; bb[5] = b0 + 1;
+  }
+  const T* tb = tab + (size_t)ring * kMfTab;
+  typedef typename V2<T>::T X2;
+  const X2* x2 = reinterpret_cast<const X2*>(x);
+  const int amax = 2 * ncr;
+  int nd[6];
+  bool ft[6], fr[6];
+  T ux[6], uz[6], fx[6], fz[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const int b = bb[k] >= B ? bb[k] - B : bb[k];
+    nd[k] = aa[k] + A * b;
+    ft[k] = dof_fixed(aa[k], b, 0, amax, pin);
+    fr[k] = dof_fixed(aa[k], b, 1, amax, pin);
+    const X2 v = x2[nd[k]];
+    const T x0 = ft[k] ? (T)0 : v.x, x1 = fr[k] ? (T)0 : v.y;
+    const T c = tb[72 + 2 * k], s = tb[73 + 2 * k];
+    ux[k] = c * x0 + s * x1;
+    uz[k] = c * x1 - s * x0;
+    fx[k] = (T)0;
+    fz[k] = (T)0;
+  }
+  const size_t st = (size_t)nel;
+  const T* D = Dw + gid;
+#pragma unroll
+  for (int ip = 0; ip < 6; ++ip) {
+    T dx[6], dz[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      dx[k] = tb[ip * 12 + k];
+      dz[k] = tb[ip * 12 + 6 + k];
+    }
+    T exx = 0, ezz = 0, gxz = 0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      exx += dx[k] * ux[k];
+      ezz += dz[k] * uz[k];
+      gxz += dz[k] * ux[k] + dx[k] * uz[k];
+    }
+    const T* Di = D + (size_t)(ip * 6) * st;
+    const T d11 = Di[0], d12 = Di[st], d13 = Di[2 * st], d22 = Di[3 * st], d23 = Di[4 * st], d33 = Di[5 * st];
+    const T sxx = d11 * exx + d12 * ezz + d13 * gxz;
+    const T szz = d12 * exx + d22 * ezz + d23 * gxz;
+    const T sxz = d13 * exx + d23 * ezz + d33 * gxz;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      fx[k] += dx[k] * sxx + dz[k] * sxz;
+      fz[k] += dz[k] * szz + dx[k] * sxz;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const T c = tb[72 + 2 * k], s = tb[73 + 2 * k];
+    const T y0 = ft[k] ? (T)0 : c * fx[k] - s * fz[k];
+    const T y1 = fr[k] ? (T)0 : s * fx[k] + c * fz[k];
+    atomic_add2(&y[2 * nd[k]], y0, y1);
+  }
+}
+
+template <typename T>
+static inline const T* mf_data(const Level& L);
+template <>
+inline const double* mf_data<double>(const Level& L) { return L.mfD64; }
+template <>
+inline const float* mf_data<float>(const Level& L) { return L.mfD32; }
+template <typename T>
+static inline const T* mf_table(const Level& L);
+template <>
+inline const double* mf_table<double>(const Level& L) { return L.mfT64; }
+template <>
+inline const float* mf_table<float>(const Level& L) { return L.mfT32; }
+
 // Grid of the tiled apply; the stacked tile only where it divides the lattice
 // exactly (ncr % (16 wr) == 0, nct % wt == 0), else the linear order.
 static void apply_tile(const Level& L, int& blocks, int& threads, int& wt) {
@@ -139,6 +239,12 @@ template void launch_apply_K<float, float>(const Level&, const float*, const flo
 // y += K x (the caller has zeroed y, typically inside the preceding vector kernel)
 template <typename Tm, typename Tv>
 void launch_apply_K_acc(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
+  if (std::is_same<Tm, Tv>::value && mf_data<Tv>(L) && mf_table<Tv>(L)) {
+    klaunch(k_apply_K_mf<Tv>, (int)div_up(L.nel, 256), 256, 0, s, mf_data<Tv>(L), mf_table<Tv>(L), x, y, L.ncr, L.nct,
+            (int)L.A(), (int)L.B(), L.pin);
+    DP_LAUNCH_CHECK();
+    return;
+  }
   int blocks, threads, wt;
   apply_tile(L, blocks, threads, wt);
   klaunch(k_apply_K<Tm, Tv>, blocks, threads, 0, s, K, x, y, (int)L.nel, L.ncr, (int)L.A(), (int)L.B(), wt);

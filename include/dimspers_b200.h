@@ -104,6 +104,10 @@ typedef struct {
                               elements run as one thread-block-cluster kernel
                               (0 = off, the default: on B200 a cluster phase
                               costs about as much as a kernel launch)        */
+  int32_t matrix_free;     /* 1 = fine-level K applies computed from the
+                              element's rotated viscous tensor at the IPs and
+                              per-ring reference shape derivatives (no packed
+                              element matrices read; default), 0 = packed    */
 } dp_solve_opts;
 
 typedef struct {
@@ -258,8 +262,8 @@ int dp_guess_from_grid(dp_ctx* ctx, const float* p_grid, int32_t nrg, int32_t nt
  * stream, from CUDA events, after an assembly: which = 0 fine-level A-apply
  * FP32, 1 fine-level A-apply FP64, 2 one multigrid V-cycle (precision of the
  * last solve).  flush_l2 = 0: `reps` back-to-back launches (warm L2);
- * 1: a 256 MB buffer is overwritten before each launch and each launch is
- * timed alone (cold L2, DRAM-bound figure). */
+ * 1: a 256 MB buffer is read before each launch and each launch is timed
+ * alone (cold L2, DRAM-bound figure). */
 int dp_profile_kernel(dp_ctx* ctx, int32_t which, int32_t reps, int32_t flush_l2, double* ms_per_launch);
 
 #ifdef __cplusplus

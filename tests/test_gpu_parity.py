@@ -203,3 +203,25 @@ def test_relaxed_inner_tolerance_accuracy():
     assert r1["status"] == 0
     assert rel(U1, U0) < 1e-7 and rel(P1, P0) < 1e-7
     assert r1["inner_iterations"] < r0["inner_iterations"]
+
+
+@pytest.mark.parametrize("pressure,kind", [("discontinuous", "aniso"), ("continuous", "fabric")])
+def test_matrix_free_apply_matches_packed_matrices(pressure, kind):
+    """The matrix-free fine-level apply (rotated tensors + per-ring reference
+    derivatives) is the operator of the packed element matrices."""
+    prob, mat, ctx = _setup(8, 64, pressure, kind)
+    with ctx:
+        ctx.set_material(mat.eta_ip, mat.rho, mat.g, mat.C6)
+        ctx.assemble(1)
+        x = np.random.default_rng(5).standard_normal(2 * ctx.nnod)
+        ys = {}
+        for mf in (0, 1):
+            ctx.solve(want_cart=False, raise_on_status=False, itmax=1, itmin=1, precision=1, matrix_free=mf)
+            ys[mf] = ctx.apply_K(x)
+        assert rel(ys[1], ys[0]) < 1e-13, rel(ys[1], ys[0])
+        out = [ctx.solve(want_cart=False, precision=p, matrix_free=mf, itmax=5000, rtol=1e-11, inner_rtol=1e-12)
+               for p in (0, 1) for mf in (0, 1)]
+    for U, P, _, r in out:
+        assert r["status"] == 0
+    for U, P, _, r in out[1:]:
+        assert rel(U, out[0][0]) < 1e-7 and rel(P, out[0][1]) < 1e-7
