@@ -91,7 +91,7 @@ struct AsmArgs {
   double* F;           // 2*nnod, accumulated with atomics (zeroed by caller)
   double* pcsum;       // npres: disc -> 1/rowsum written; cont -> rowsum accumulated
   double* Minv;        // 6*nel: inverse of the element mass block (discontinuous pressure)
-  double* mfD;         // 36*nel or null: omega * Q^T D Q per IP, ring-major (matrix-free apply)
+  double* mfD;         // 36*nel or null: omega * Q^T D Q per IP, entry-major (matrix-free apply)
   CartOut cart;
 };
 
@@ -158,8 +158,7 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs p) {
   // rotated by phi = theta(v0) - theta(v0 of the reference); its polar operator
   // is sum_ip om B0^T (Q^T D Q) B0 with Q the engineering-strain rotation by phi
   double qc = 1.0, qs = 0.0;
-  const int ering = 2 * ir + t;                   // ring-major index of the element
-  const size_t emf = (size_t)ering * p.nct + it;
+  const size_t emf = (size_t)e;
   if (p.mfD) {
     const int bref = (t == 0) ? 0 : 2;            // vertex 0 of the reference element
     sincos(th[0] - p.theta_lat[2 * ir + p.A * bref], &qs, &qc);
@@ -358,10 +357,12 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs p) {
 #undef ACC
 }
 
-// Per ring (ir, t) of the matrix-free apply: the reference element's (it = 0)
-// Cartesian shape-function derivatives at the 6 IPs and its node rotations:
-// tab[ring * 84 + ip * 12 + k] = dN_k/dx, [.. + 6 + k] = dN_k/dz, [ring * 84 +
-// 72 + 2k] = cos theta_k, [.. + 1] = sin theta_k.  Same formulas as k_assemble.
+// Per ring (ir, t) of the matrix-free apply (ring = 2 ir + t): the reference
+// element's (it = 0) Cartesian shape-function derivatives at the 6 IPs and its
+// node rotations, value-major so that consecutive rings are consecutive:
+// tab[(ip * 12 + k) * nring + ring] = dN_k/dx, [(ip * 12 + 6 + k) * nring + ring]
+// = dN_k/dz, [(72 + 2k) * nring + ring] = cos theta_k, [(73 + 2k) ..] = sin.
+// Same formulas as k_assemble.
 __global__ void k_mf_table(int ncr, int A, const double* __restrict__ theta_lat, const double* __restrict__ r_lat,
                            double* __restrict__ tab) {
   const int ring = blockIdx.x * blockDim.x + threadIdx.x;
@@ -390,7 +391,8 @@ __global__ void k_mf_table(int ncr, int A, const double* __restrict__ theta_lat,
   const double detJ = Jt0 * Jr1 - Jt1 * Jr0;
   const double R31 = rr[2] - rr[0], R21 = rr[1] - rr[0];
   const double T31 = th[2] - th[0], T21 = th[1] - th[0];
-  double* o = tab + (size_t)ring * kMfTab;
+  const int nring = 2 * ncr;
+  double* o = tab + ring;
   for (int ip = 0; ip < 6; ++ip) {
     const double th_ip = th[0] * c_N3[ip][0] + th[1] * c_N3[ip][1] + th[2] * c_N3[ip][2];
     const double r_ip = rr[0] * c_N3[ip][0] + rr[1] * c_N3[ip][1] + rr[2] * c_N3[ip][2];
@@ -402,15 +404,15 @@ __global__ void k_mf_table(int ncr, int A, const double* __restrict__ theta_lat,
     const double iz0 = (-R31 * s - T31 * c * r_ip) * inv;
     const double iz1 = (R21 * s + T21 * c * r_ip) * inv;
     for (int k = 0; k < 6; ++k) {
-      o[ip * 12 + k] = ix0 * c_dN[ip][0][k] + ix1 * c_dN[ip][1][k];
-      o[ip * 12 + 6 + k] = iz0 * c_dN[ip][0][k] + iz1 * c_dN[ip][1][k];
+      o[(size_t)(ip * 12 + k) * nring] = ix0 * c_dN[ip][0][k] + ix1 * c_dN[ip][1][k];
+      o[(size_t)(ip * 12 + 6 + k) * nring] = iz0 * c_dN[ip][0][k] + iz1 * c_dN[ip][1][k];
     }
   }
   for (int k = 0; k < 6; ++k) {
     double s, c;
     sincos(theta_lat[nd[k]], &s, &c);
-    o[72 + 2 * k] = c;
-    o[72 + 2 * k + 1] = s;
+    o[(size_t)(72 + 2 * k) * nring] = c;
+    o[(size_t)(73 + 2 * k) * nring] = s;
   }
 }
 

@@ -186,7 +186,17 @@ static void set_fine_apply(Ctx& c, const SolveCfg& cfg) {
   c.fine.warps_t = cfg.mg.apply_warps_t;
   c.fine.mfD64 = c.fine.mfT64 = nullptr;
   c.fine.mfD32 = c.fine.mfT32 = nullptr;
-  if (!cfg.matrix_free || !c.mfD64) return;
+  if (!cfg.matrix_free) return;
+  if (!c.mfD64) {
+    // first matrix-free solve on this context: allocate the data and assemble
+    // again to fill it (every later assembly keeps it current)
+    dalloc(&c.mfD64, 36 * c.fine.nel);
+    dalloc(&c.mfT64, (int64_t)kMfTab * 2 * c.fine.ncr);
+    const int keep = c.assembled;
+    launch_assemble(c, c.assembled >= 1 ? 1 : 0, nullptr);
+    c.assembled = keep;
+    c.mf32_stale = true;
+  }
   c.fine.mfD64 = c.mfD64;
   c.fine.mfT64 = c.mfT64;
   if (cfg.precision >= 1) {
@@ -361,7 +371,7 @@ void dp_default_opts(dp_solve_opts* o) {
   o->apply_warps_t = 1;
   o->launch_overlap = 1;
   o->mg_tail = 0;
-  o->matrix_free = 1;
+  o->matrix_free = 0;
 }
 
 const char* dp_status_string(int s) {
@@ -593,11 +603,7 @@ int dp_assemble(dp_ctx* h, int32_t precision) {
       dalloc(&c.K32, kstore<float>(c.fine.nel));
       DP_CUDA(cudaMemset(c.K32, 0, sizeof(float) * kstore<float>(c.fine.nel)));
     }
-    if (!c.mfD64) {
-      dalloc(&c.mfD64, 36 * c.fine.nel);
-      dalloc(&c.mfT64, (int64_t)kMfTab * 2 * c.fine.ncr);
-    }
-    launch_assemble(c, precision, nullptr);
+    launch_assemble(c, precision, nullptr);  // also refreshes the matrix-free data once enabled
     c.mf32_stale = true;
     c.assembled = precision;
     c.mg_prec = c.mg.empty() ? -1 : c.mg_prec;  // hierarchy values are rebuilt on the next solve

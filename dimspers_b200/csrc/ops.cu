@@ -121,9 +121,10 @@ __global__ void __launch_bounds__(256) k_apply_K(const Tm* __restrict__ K, const
 // (written by the assembly).  Per element the apply reads 36 Dw values (144 B
 // in FP32 instead of 312 B of packed matrix) and does ~400 FMA: node DOFs to
 // the reference Cartesian frame, strain (exx, ezz, gxz) per IP, stress = Dw
-// strain, back-projection, back to polar.  Threads run along theta (ring-
-// major element order), so a warp shares its ring: the table reads are warp-
-// uniform and the Dw reads are coalesced.
+// strain, back-projection, back to polar.  Threads run along r (the element
+// order of the packed apply), so node gathers and atomics are contiguous; the
+// per-ring table is value-major, so the lanes of a warp (consecutive rings)
+// read it with coalesced loads.
 template <typename T>
 __global__ void __launch_bounds__(256) k_apply_K_mf(const T* __restrict__ Dw, const T* __restrict__ tab,
                                                     const T* __restrict__ x, T* __restrict__ y, int ncr, int nct,
@@ -132,8 +133,9 @@ __global__ void __launch_bounds__(256) k_apply_K_mf(const T* __restrict__ Dw, co
   const int nel = 2 * ncr * nct;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= nel) return;
-  const int it = gid % nct, ring = gid / nct;
-  const int ir = ring >> 1, t = ring & 1;
+  const int q = gid >> 1, t = gid & 1;
+  const int ir = q % ncr, it = q / ncr;
+  const int ring = 2 * ir + t, nring = 2 * ncr;
   const int a0 = 2 * ir, b0 = 2 * it;
   int aa[6], bb[6];
   if (t == 0) {
@@ -143,7 +145,7 @@ __global__ void __launch_bounds__(256) k_apply_K_mf(const T* __restrict__ Dw, co
     aa[0] = a0; aa[1] = a0 + 2; aa[2] = a0 + 2; aa[3] = a0 + 1; aa[4] = a0 + 2; aa[5] = a0 + 1;
     bb[0] = b0 + 2; bb[1] = b0 + 2; bb[2] = b0; bb[3] = b0 + 2; bb[4] = b0 + 1; bb[5] = b0 + 1;
   }
-  const T* tb = tab + (size_t)ring * kMfTab;
+  const T* tb = tab + ring;
   typedef typename V2<T>::T X2;
   const X2* x2 = reinterpret_cast<const X2*>(x);
   const int amax = 2 * ncr;
@@ -158,7 +160,7 @@ __global__ void __launch_bounds__(256) k_apply_K_mf(const T* __restrict__ Dw, co
     fr[k] = dof_fixed(aa[k], b, 1, amax, pin);
     const X2 v = x2[nd[k]];
     const T x0 = ft[k] ? (T)0 : v.x, x1 = fr[k] ? (T)0 : v.y;
-    const T c = tb[72 + 2 * k], s = tb[73 + 2 * k];
+    const T c = __ldg(tb + (72 + 2 * k) * nring), s = __ldg(tb + (73 + 2 * k) * nring);
     ux[k] = c * x0 + s * x1;
     uz[k] = c * x1 - s * x0;
     fx[k] = (T)0;
@@ -166,35 +168,41 @@ __global__ void __launch_bounds__(256) k_apply_K_mf(const T* __restrict__ Dw, co
   }
   const size_t st = (size_t)nel;
   const T* D = Dw + gid;
+  // the IP loop stays rolled (the table is read per IP, warp-uniform, from
+  // L1) and the next IP's six tensor values are loaded one IP ahead
+  T dn[6];
 #pragma unroll
+  for (int v = 0; v < 6; ++v) dn[v] = D[v * st];
+#pragma unroll 1
   for (int ip = 0; ip < 6; ++ip) {
-    T dx[6], dz[6];
+    const T d11 = dn[0], d12 = dn[1], d13 = dn[2], d22 = dn[3], d23 = dn[4], d33 = dn[5];
+    if (ip < 5) {
+      const T* Dn = D + (size_t)((ip + 1) * 6) * st;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      dx[k] = tb[ip * 12 + k];
-      dz[k] = tb[ip * 12 + 6 + k];
+      for (int v = 0; v < 6; ++v) dn[v] = Dn[v * st];
     }
+    const T* tq = tb + ip * 12 * nring;
     T exx = 0, ezz = 0, gxz = 0;
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      exx += dx[k] * ux[k];
-      ezz += dz[k] * uz[k];
-      gxz += dz[k] * ux[k] + dx[k] * uz[k];
+      const T dxk = __ldg(tq + k * nring), dzk = __ldg(tq + (6 + k) * nring);
+      exx += dxk * ux[k];
+      ezz += dzk * uz[k];
+      gxz += dzk * ux[k] + dxk * uz[k];
     }
-    const T* Di = D + (size_t)(ip * 6) * st;
-    const T d11 = Di[0], d12 = Di[st], d13 = Di[2 * st], d22 = Di[3 * st], d23 = Di[4 * st], d33 = Di[5 * st];
     const T sxx = d11 * exx + d12 * ezz + d13 * gxz;
     const T szz = d12 * exx + d22 * ezz + d23 * gxz;
     const T sxz = d13 * exx + d23 * ezz + d33 * gxz;
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      fx[k] += dx[k] * sxx + dz[k] * sxz;
-      fz[k] += dz[k] * szz + dx[k] * sxz;
+      const T dxk = __ldg(tq + k * nring), dzk = __ldg(tq + (6 + k) * nring);
+      fx[k] += dxk * sxx + dzk * sxz;
+      fz[k] += dzk * szz + dxk * sxz;
     }
   }
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
-    const T c = tb[72 + 2 * k], s = tb[73 + 2 * k];
+    const T c = __ldg(tb + (72 + 2 * k) * nring), s = __ldg(tb + (73 + 2 * k) * nring);
     const T y0 = ft[k] ? (T)0 : c * fx[k] - s * fz[k];
     const T y1 = fr[k] ? (T)0 : s * fx[k] + c * fz[k];
     atomic_add2(&y[2 * nd[k]], y0, y1);

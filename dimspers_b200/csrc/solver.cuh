@@ -22,7 +22,7 @@ struct SolveCfg {
   double inner_relax = 0.0; // > 0: relaxed inner tolerance with this cap
   int schur_pc = 0;         // 0 lumped mass (StokesPcCG), 1 element-block mass inverse
   int launch_overlap = 1;   // 1: programmatic dependent launch between solver kernels
-  int matrix_free = 1;      // 1: fine-level applies from the rotated tensors (no element matrices)
+  int matrix_free = 0;      // 1: fine-level applies from the rotated tensors (no element matrices)
   MGOptions mg;
 };
 

@@ -106,8 +106,10 @@ typedef struct {
                               costs about as much as a kernel launch)        */
   int32_t matrix_free;     /* 1 = fine-level K applies computed from the
                               element's rotated viscous tensor at the IPs and
-                              per-ring reference shape derivatives (no packed
-                              element matrices read; default), 0 = packed    */
+                              per-ring reference shape derivatives (144 B per
+                              element read instead of 312; slower on B200, where
+                              the packed apply runs near HBM peak), 0 = packed
+                              element matrices (default)                      */
 } dp_solve_opts;
 
 typedef struct {
