@@ -33,7 +33,7 @@ class SolveOpts(C.Structure):
                 ("coarse_max", C.c_int32), ("schur_pc", C.c_int32),
                 ("apply_warps", C.c_int32), ("apply_warps_t", C.c_int32),
                 ("launch_overlap", C.c_int32), ("mg_tail", C.c_int32),
-                ("matrix_free", C.c_int32)]
+                ("matrix_free", C.c_int32), ("cheb_degree_coarse", C.c_int32), ("true_residual", C.c_int32)]
 
 
 class SolveReport(C.Structure):
@@ -42,7 +42,7 @@ class SolveReport(C.Structure):
                 ("div_residual", C.c_double), ("mom_residual", C.c_double),
                 ("t_assemble_ms", C.c_double), ("t_setup_ms", C.c_double), ("t_solve_ms", C.c_double),
                 ("fallback_used", C.c_int32), ("mg_levels", C.c_int32), ("kernel_launches", C.c_int64),
-                ("refinements", C.c_int64), ("r0_guess", C.c_double)]
+                ("refinements", C.c_int64), ("r0_guess", C.c_double), ("restarts", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -109,6 +109,8 @@ static SolveCfg make_cfg(const dp_solve_opts* o) {
   cfg.use_guess = o->use_guess;
   cfg.verbose = o->verbose;
   if (o->cheb_degree > 0) cfg.mg.cheb_degree = o->cheb_degree;
+  if (o->cheb_degree_coarse < 0) throw BadArg("cheb_degree_coarse must be >= 0");
+  cfg.mg.cheb_degree_coarse = o->cheb_degree_coarse;
   if (o->inner_rtol32 > 0) cfg.inner_rtol32 = o->inner_rtol32;
   if (o->max_refine > 0) cfg.max_refine = o->max_refine;
   cfg.host_loop = o->host_loop;
@@ -127,6 +129,8 @@ static SolveCfg make_cfg(const dp_solve_opts* o) {
   cfg.launch_overlap = o->launch_overlap;
   if (o->matrix_free != 0 && o->matrix_free != 1) throw BadArg("matrix_free must be 0 or 1");
   cfg.matrix_free = o->matrix_free;
+  if (o->true_residual != 0 && o->true_residual != 1) throw BadArg("true_residual must be 0 or 1");
+  cfg.true_residual = o->true_residual;
   if (o->mg_tail < 0) throw BadArg("mg_tail must be 0 (off) or a positive element count");
   cfg.mg.tail_max_el = o->mg_tail;
   if (o->apply_warps > 0) cfg.mg.apply_warps = o->apply_warps;
@@ -263,6 +267,7 @@ static void fill_report(const Ctx& c, const SolveResult& res, dp_solve_report* r
   rep->refinements = res.refinements;
   rep->fallback_used = res.fallback;
   rep->r0_guess = res.r0_guess;
+  rep->restarts = res.restarts;
 }
 
 }  // namespace dp
@@ -372,6 +377,7 @@ void dp_default_opts(dp_solve_opts* o) {
   o->launch_overlap = 1;
   o->mg_tail = 0;
   o->matrix_free = 0;
+  o->true_residual = 1;
 }
 
 const char* dp_status_string(int s) {

@@ -68,6 +68,7 @@ struct MGLevel {
   double* dinv64 = nullptr;  // 3*nnod inverse of the 2x2 nodal diagonal blocks (i00, i01, i11)
   float* dinv32 = nullptr;
   double lmax = 0.0;         // estimate of lambda_max(D^-1 A)
+  int degree = 3;            // Chebyshev steps on this level
   double* cheb = nullptr;    // device: [1/theta, -, (c1, c2) per further step]
   // work vectors (precision of the hierarchy)
   void* x = nullptr;
@@ -133,7 +134,7 @@ struct Ctx {
   // graph-captured solve (graph.cu)
   void* ctl = nullptr;          // device control block (DevCtl)
   void* h_ctl = nullptr;        // pinned host mirror
-  cudaStream_t aux[3] = {nullptr, nullptr, nullptr};  // capture streams of nested loop bodies
+  cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};  // capture streams of nested loop bodies
   void* graph = nullptr;        // cudaGraph_t
   void* gexec = nullptr;        // cudaGraphExec_t
   int64_t gkey = -1;
@@ -142,7 +143,7 @@ struct Ctx {
   const void* gP = nullptr;
   int64_t gk_main = 0;          // kernel nodes outside loop bodies
   int64_t cap_nested = 0;       // kernels captured inside nested bodies (capture bookkeeping)
-  int64_t gk_body[4] = {0, 0, 0, 0};  // kernel nodes per body execution (outer, pcg64, pcg32, refinement)
+  int64_t gk_body[5] = {0, 0, 0, 0, 0};  // kernel nodes per body execution (outer, pcg64, pcg32, refinement, restart)
 
   ~Ctx();
 };

@@ -30,7 +30,7 @@ struct DevCtl {
   double rtol, inner_rtol, inner_rtol32, relax_cap;
   int itmax, itmin, inner_itmax, max_refine;
   // state
-  int outer_it, in_it, in32_it, ref_it, status, guess_used;
+  int outer_it, in_it, in32_it, ref_it, status, guess_used, restarts, max_restarts;
   long long in_total, in32_total, ref_total;
   double r0, tol, in_tol2, in32_tol2, ref_tol2, r0ref, r0guess;
 };
@@ -108,6 +108,51 @@ __global__ void k_outer_check(cudaGraphConditionalHandle h, DevCtl* ctl, const d
     go = 0u;
   } else if (it >= ctl->itmax) {
     go = 0u;
+  }
+  cudaGraphSetConditional(h, go);
+}
+
+// ---- true-residual restarts ------------------------------------------------------
+// With relaxed (inexact) inner solves the outer residual r, updated by
+// recurrence, drifts from the true Schur residual -G^T K^-1 (F + G P), and U
+// (accumulated from inexact solves) from K^-1 (F + G P).  In the restart mode
+// the outer loop runs inside a second WHILE loop: when it stops, U is solved
+// afresh to the tight inner tolerance, the true residual is formed, and the
+// loop restarts from the current P (same r0, same iteration count) unless the
+// true residual meets the tolerance.
+__global__ void k_outer_start(DevCtl* ctl, const double* scal, int use_ref) {
+  grid_dep_wait();
+  const double r0 = use_ref ? ctl->r0ref : sqrt(scal[S_RR]);
+  ctl->r0 = r0;
+  ctl->tol = r0 * ctl->rtol;
+  ctl->outer_it = 0;
+  ctl->restarts = 0;
+  ctl->status = r0 > 0.0 ? 1 : 0;
+}
+__global__ void k_restart_init(cudaGraphConditionalHandle h, const DevCtl* ctl) {
+  grid_dep_wait();
+  cudaGraphSetConditional(h, (ctl->r0 > 0.0 && ctl->itmax >= 1) ? 1u : 0u);
+}
+// outer loop (re)entry: continue while the current (true) residual misses the tolerance
+__global__ void k_outer_resume(cudaGraphConditionalHandle h, DevCtl* ctl, const double* scal) {
+  grid_dep_wait();
+  const double rn = sqrt(scal[S_RR]);
+  const bool done = (rn < ctl->tol && ctl->outer_it >= ctl->itmin) || ctl->outer_it >= ctl->itmax;
+  ctl->status = done ? (rn < ctl->tol ? 0 : 1) : 1;
+  cudaGraphSetConditional(h, done ? 0u : 1u);
+}
+__global__ void k_restart_check(cudaGraphConditionalHandle h, DevCtl* ctl, const double* scal) {
+  grid_dep_wait();
+  ctl->restarts += 1;
+  const double rn = sqrt(scal[S_RR]);
+  unsigned go = 0u;
+  if (ctl->status == 2) {
+    go = 0u;                                   // breakdown
+  } else if (rn < ctl->tol && ctl->outer_it >= ctl->itmin) {
+    ctl->status = 0;
+  } else {
+    ctl->status = 1;
+    go = (ctl->outer_it < ctl->itmax && ctl->restarts <= ctl->max_restarts) ? 1u : 0u;
   }
   cudaGraphSetConditional(h, go);
 }
@@ -275,7 +320,7 @@ static cudaGraph_t add_while(cudaStream_t s, cudaGraphConditionalHandle h) {
 }
 
 // Loop bodies by role, for the launch count: kernels per execution of each body.
-enum BodyRole { B_OUTER = 0, B_PCG64 = 1, B_PCG32 = 2, B_REF = 3 };
+enum BodyRole { B_OUTER = 0, B_PCG64 = 1, B_PCG32 = 2, B_REF = 3, B_RESTART = 4 };
 
 // Captures emit() into body on the auxiliary stream of the given depth.
 template <typename F>
@@ -406,51 +451,82 @@ static void emit_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
     klaunch(k_sub_mean, g_nb(nP), 256, 0, c.stream, rz, nP, c.scal + S_SUMR);
     launch_dot(c, rz, rz, nP, G_RZREF);
   }
-  // Rhs = F + G P ; U = K^-1 Rhs
-  if (!cfg.use_guess) DP_CUDA(cudaMemsetAsync(P, 0, sizeof(double) * nP, c.stream));
-  launch_apply_G(c, P, y);
-  klaunch(k_add, g_nb(nU), 256, 0, c.stream, c.F, y, rhs, nU);
-  emit_inner(c, cfg, rhs, U, 0, 0);
-  // r = -G^T U ; rm0space!(r) ; ||r0||
-  launch_apply_GT(c, U, r);
-  klaunch(k_neg, g_nb(nP), 256, 0, c.stream, r, nP);
-  launch_sum(c, r, nP, S_SUMR);
-  klaunch(k_sub_mean, g_nb(nP), 256, 0, c.stream, r, nP, c.scal + S_SUMR);
-  launch_dot(c, r, r, nP, S_RR);
-  if (cfg.use_guess == 2) {
-    klaunch(k_guess_select, 1, 1, 0, c.stream, ctl, c.scal);
-    klaunch(k_guess_apply, g_nb(std::max(nU, nP)), 256, 0, c.stream, ctl, U, (const double*)c.work[W_UC], r,
-                                                                  (const double*)c.work[W_RLAST], P, nU, nP);
-  }
+  // Rhs = F + G P ; U = K^-1 Rhs (tight inner tolerance) ; r = -G^T U ;
+  // rm0space!(r) ; ||r||^2 -> S_RR.  The initial residual, and in the restart
+  // mode the true residual after each pass of the outer loop.
+  auto true_residual = [&](int depth) {
+    launch_apply_G(c, P, y);
+    klaunch(k_add, g_nb(nU), 256, 0, c.stream, c.F, y, rhs, nU);
+    emit_inner(c, cfg, rhs, U, depth, 0);
+    launch_apply_GT(c, U, r);
+    klaunch(k_neg, g_nb(nP), 256, 0, c.stream, r, nP);
+    launch_sum(c, r, nP, S_SUMR);
+    klaunch(k_sub_mean, g_nb(nP), 256, 0, c.stream, r, nP, c.scal + S_SUMR);
+    launch_dot(c, r, r, nP, S_RR);
+  };
   // d = r .* pc (or M^-1 r) ; q = d
-  if (cfg.schur_pc == 1) {
-    klaunch(k_mass_blk, g_nb(L.nel), 256, 0, c.stream, r, c.Minv, d, (int)L.nel);
-  } else {
-    klaunch(k_mul_into, g_nb(nP), 256, 0, c.stream, r, c.pc, d, nP);
-  }
-  DP_CUDA(cudaMemcpyAsync(q, d, sizeof(double) * nP, cudaMemcpyDeviceToDevice, c.stream));
-  launch_sum(c, q, nP, S_SUMQ);
-  cudaGraphConditionalHandle h = new_handle(c.stream);
-  klaunch(k_outer_init, 1, 1, 0, c.stream, h, ctl, c.scal, cfg.use_guess == 2 ? 1 : 0);
-  DP_LAUNCH_CHECK();
-  cudaGraph_t body = add_while(c.stream, h);
-  capture_body(c, body, 0, B_OUTER, [&] {
+  auto pc_start = [&] {
+    if (cfg.schur_pc == 1) {
+      klaunch(k_mass_blk, g_nb(L.nel), 256, 0, c.stream, r, c.Minv, d, (int)L.nel);
+    } else {
+      klaunch(k_mul_into, g_nb(nP), 256, 0, c.stream, r, c.pc, d, nP);
+    }
+    DP_CUDA(cudaMemcpyAsync(q, d, sizeof(double) * nP, cudaMemcpyDeviceToDevice, c.stream));
+    launch_sum(c, q, nP, S_SUMQ);
+  };
+  // the StokesPcCG iteration (IterativeSolvers.jl:130-166) as a WHILE body
+  auto outer_body = [&](cudaGraphConditionalHandle h, int depth) {
     klaunch(k_q_center_rd, red_grid(nP), kRedThreads, 0, c.stream, q, r, d, nP, c.scal, c.partial, c.counter);
     launch_apply_G(c, q, y);
-    emit_inner(c, cfg, y, z, 1, cfg.inner_relax > 0.0 ? 1 : 0);
+    emit_inner(c, cfg, y, z, depth + 1, cfg.inner_relax > 0.0 ? 1 : 0);
     launch_apply_GT(c, z, Sq);
     launch_dot(c, q, Sq, nP, S_QSQ);
-    klaunch(k_schur_update_p, red_grid(nP), kRedThreads, 0, c.stream, P, r, rlast, q, Sq, nP, c.scal, c.partial, c.counter);
+    klaunch(k_schur_update_p, red_grid(nP), kRedThreads, 0, c.stream, P, r, rlast, q, Sq, nP, c.scal, c.partial,
+            c.counter);
     klaunch(k_axpy_slot, g_nb(nU), 256, 0, c.stream, U, z, nU, c.scal);
     if (cfg.schur_pc == 1)
       klaunch(k_schur_center_blk, red_grid(L.nel), kRedThreads, 0, c.stream, r, rlast, c.Minv, d, (int)L.nel, c.scal,
-                                                                         c.partial, c.counter);
+              c.partial, c.counter);
     else
-      klaunch(k_schur_center, red_grid(nP), kRedThreads, 0, c.stream, r, rlast, c.pc, d, nP, c.scal, c.partial, c.counter);
+      klaunch(k_schur_center, red_grid(nP), kRedThreads, 0, c.stream, r, rlast, c.pc, d, nP, c.scal, c.partial,
+              c.counter);
     klaunch(k_q_update, red_grid(nP), kRedThreads, 0, c.stream, q, d, nP, c.scal, c.partial, c.counter);
     klaunch(k_outer_check, 1, 1, 0, c.stream, h, ctl, c.scal);
     DP_LAUNCH_CHECK();
-  });
+  };
+
+  if (!cfg.use_guess) DP_CUDA(cudaMemsetAsync(P, 0, sizeof(double) * nP, c.stream));
+  true_residual(0);
+  if (cfg.use_guess == 2) {
+    klaunch(k_guess_select, 1, 1, 0, c.stream, ctl, c.scal);
+    klaunch(k_guess_apply, g_nb(std::max(nU, nP)), 256, 0, c.stream, ctl, U, (const double*)c.work[W_UC], r,
+            (const double*)c.work[W_RLAST], P, nU, nP);
+  }
+  if (!cfg.true_residual) {
+    pc_start();
+    cudaGraphConditionalHandle h = new_handle(c.stream);
+    klaunch(k_outer_init, 1, 1, 0, c.stream, h, ctl, c.scal, cfg.use_guess == 2 ? 1 : 0);
+    DP_LAUNCH_CHECK();
+    cudaGraph_t body = add_while(c.stream, h);
+    capture_body(c, body, 0, B_OUTER, [&] { outer_body(h, 0); });
+  } else {
+    klaunch(k_outer_start, 1, 1, 0, c.stream, ctl, c.scal, cfg.use_guess == 2 ? 1 : 0);
+    cudaGraphConditionalHandle hr = new_handle(c.stream);
+    klaunch(k_restart_init, 1, 1, 0, c.stream, hr, ctl);
+    DP_LAUNCH_CHECK();
+    cudaGraph_t rbody = add_while(c.stream, hr);
+    capture_body(c, rbody, 0, B_RESTART, [&] {
+      pc_start();
+      cudaGraphConditionalHandle h = new_handle(c.stream);
+      klaunch(k_outer_resume, 1, 1, 0, c.stream, h, ctl, c.scal);
+      DP_LAUNCH_CHECK();
+      cudaGraph_t body = add_while(c.stream, h);
+      capture_body(c, body, 1, B_OUTER, [&] { outer_body(h, 1); });
+      true_residual(1);
+      klaunch(k_restart_check, 1, 1, 0, c.stream, hr, ctl, c.scal);
+      DP_LAUNCH_CHECK();
+    });
+  }
   // diagnostics on the raw solution
   launch_apply_K<double, double>(L, c.K64, U, rhs, c.stream);
   launch_apply_G(c, P, y);
@@ -472,12 +548,13 @@ static void emit_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
 
 static int64_t graph_key(const SolveCfg& cfg, const Ctx& c) {
   return (int64_t)cfg.precision | ((int64_t)cfg.inner_pc << 2) | ((int64_t)cfg.use_guess << 3) |
-         ((int64_t)cfg.remove_rotation << 5) | ((int64_t)c.mg_degree << 6) | ((int64_t)c.mg.size() << 10) |
+         ((int64_t)cfg.remove_rotation << 5) | ((int64_t)c.mg_degree << 40) | ((int64_t)c.mg.size() << 10) |
          ((int64_t)(cfg.inner_relax > 0.0) << 15) | ((int64_t)c.mg_prec << 16) | ((int64_t)cfg.schur_pc << 18) |
          ((int64_t)cfg.mg.block_jacobi << 20) | ((int64_t)(c.coarse_n > 0) << 21) |
          ((int64_t)cfg.mg.apply_warps << 24) | ((int64_t)cfg.mg.apply_warps_t << 28) |
          ((int64_t)cfg.launch_overlap << 32) | ((int64_t)tail_start(c, cfg.mg) << 33) |
-         ((int64_t)cfg.matrix_free << 37);
+         ((int64_t)cfg.matrix_free << 37) |
+         ((int64_t)cfg.true_residual << 38);
 }
 
 void graph_free(Ctx& c) {
@@ -492,7 +569,7 @@ static void ensure_ctl(Ctx& c) {
   if (!c.ctl) {
     DP_CUDA(cudaMalloc(&c.ctl, sizeof(DevCtl)));
     DP_CUDA(cudaMallocHost(&c.h_ctl, sizeof(DevCtl)));
-    for (int i = 0; i < 3; ++i) DP_CUDA(cudaStreamCreateWithFlags(&c.aux[i], cudaStreamNonBlocking));
+    for (int i = 0; i < 4; ++i) DP_CUDA(cudaStreamCreateWithFlags(&c.aux[i], cudaStreamNonBlocking));
   }
 }
 
@@ -516,6 +593,7 @@ static void upload_params(Ctx& c, const SolveCfg& cfg, cudaStream_t s) {
   h.itmin = cfg.itmin;
   h.inner_itmax = cfg.inner_itmax;
   h.max_refine = cfg.max_refine;
+  h.max_restarts = cfg.max_restarts;
   *(DevCtl*)c.h_ctl = h;
   DP_CUDA(cudaMemcpyAsync(c.ctl, c.h_ctl, sizeof(DevCtl), cudaMemcpyHostToDevice, s));
 }
@@ -535,7 +613,9 @@ static void collect_result(Ctx& c, const SolveCfg& cfg, cudaStream_t s, SolveRes
   res.omega = cfg.remove_rotation ? c.h_scal[S_AM] / c.h_scal[S_MOM] : 0.0;
   res.inner_its = cfg.precision == 2 ? o.in32_total : o.in_total;
   res.launches = c.gk_main + c.gk_body[B_OUTER] * o.outer_it + c.gk_body[B_PCG64] * o.in_total +
-                 c.gk_body[B_PCG32] * o.in32_total + c.gk_body[B_REF] * o.ref_total;
+                 c.gk_body[B_PCG32] * o.in32_total + c.gk_body[B_REF] * o.ref_total +
+                 (cfg.true_residual ? c.gk_body[B_RESTART] * o.restarts : 0);
+  res.restarts = cfg.true_residual ? o.restarts : 1;
   res.refinements = o.ref_total;
   res.fallback = (cfg.use_guess == 2) ? (o.guess_used ? 0 : 1) : 0;
   res.r0_guess = o.r0guess;

@@ -735,8 +735,10 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
   double* diag = nullptr;
   DP_CUDA(cudaMalloc(&diag, sizeof(double) * 3 * c.mg[0].g.nnod));
   const int deg = std::max(1, std::min(o.cheb_degree, kMaxCheb));
+  const int deg_coarse = o.cheb_degree_coarse > 0 ? std::max(1, std::min(o.cheb_degree_coarse, kMaxCheb)) : deg;
   for (size_t l = 0; l < c.mg.size(); ++l) {
     MGLevel& L = c.mg[l];
+    L.degree = l == 0 ? deg : deg_coarse;
     DP_CUDA(cudaMemsetAsync(diag, 0, sizeof(double) * 3 * L.g.nnod, c.stream));
     klaunch(k_diag_blocks<T>, (int)div_up(L.g.nel, 128), 128, 0, c.stream, level_K<T>(L), diag, (int)L.g.nel, L.g.ncr,
                                                                        (int)L.g.A(), (int)L.g.B());
@@ -752,7 +754,7 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
       const double theta = 0.5 * (lmx + lmn), delta = 0.5 * (lmx - lmn), sigma = theta / delta;
       double rho_prev = 1.0 / sigma;
       coef[0] = 1.0 / theta;
-      for (int k = 1; k < deg; ++k) {
+      for (int k = 1; k < L.degree; ++k) {
         const double rho = 1.0 / (2.0 * sigma - rho_prev);
         coef[2 * k] = rho * rho_prev;
         coef[2 * k + 1] = 2.0 * rho / delta;
@@ -762,7 +764,7 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
     DP_CUDA(cudaMemcpyAsync(L.cheb, coef, sizeof(coef), cudaMemcpyHostToDevice, c.stream));
     DP_CUDA(cudaStreamSynchronize(c.stream));
   }
-  c.mg_degree = deg;
+  c.mg_degree = deg + 16 * deg_coarse;  // both degrees shape the captured graph
   DP_CUDA(cudaFree(diag));
   // coarse dense inverse
   if (c.coarse_n > 0) {
@@ -806,7 +808,7 @@ static void chebyshev(Ctx& c, MGLevel& L, const T* b, T* x, int mode) {
     launch_apply_K_acc<T, T>(L.g, level_K<T>(L), x, r, c.stream);
     klaunch(k_cheb_first_x<T>, tpb(nn), 256, 0, c.stream, b, dinv, x, r, d, Ad, L.cheb, nn);
   }
-  for (int k = 1; k < c.mg_degree; ++k) {
+  for (int k = 1; k < L.degree; ++k) {
     launch_apply_K_acc<T, T>(L.g, level_K<T>(L), d, Ad, c.stream);
     klaunch(k_cheb_step<T>, tpb(nn), 256, 0, c.stream, Ad, dinv, x, r, d, L.cheb + 2 * k, nn);
   }

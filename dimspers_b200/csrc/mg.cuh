@@ -8,6 +8,7 @@ constexpr int kMaxCheb = 8;
 
 struct MGOptions {
   int cheb_degree = 3;      // Chebyshev steps per smoothing (each one A-apply)
+  int cheb_degree_coarse = 0;  // on the levels below the finest (0: cheb_degree)
   double cheb_lo = 0.15;    // smoothing interval [lo, hi] * lambda_max(D^-1 A)
   double cheb_hi = 1.1;
   int block_jacobi = 1;     // 1: 2x2 nodal blocks (u_theta, u_r); 0: point Jacobi

@@ -40,13 +40,13 @@ struct TailLevel {
   const double* cheb;   // Chebyshev recurrence coefficients
   T *x, *b, *r, *d, *t; // level vectors (2 per node)
   int ncr, nct, pin, nel, nnod, A, B;
+  int degree;           // Chebyshev steps on this level
 };
 
 template <typename T>
 struct TailArgs {
   TailLevel<T> L[kTailMaxLevels];
   int nlev;            // tail levels; the last is the coarsest
-  int degree;          // Chebyshev degree
   int first_done;      // top level: the first smoothing step was fused into the restriction
   const double* inv;   // dense inverse of the coarsest level (ninv x ninv), or null
   int ninv;
@@ -116,7 +116,7 @@ __device__ __forceinline__ void tail_cheb_step(const TailLevel<T>& L, const doub
 // Chebyshev smoothing on level L (the phases of chebyshev() in mg.cu).
 // mode 0: from x = 0; 1: from x = 0, first step already taken; 2: from x (r zero on entry).
 template <typename T>
-__device__ void tail_smooth(const TailLevel<T>& L, int mode, int degree, cg::cluster_group& cl, int tid, int nth) {
+__device__ void tail_smooth(const TailLevel<T>& L, int mode, cg::cluster_group& cl, int tid, int nth) {
   if (mode == 0) {
     tail_cheb_first(L, tid, nth);
     cl.sync();
@@ -126,7 +126,7 @@ __device__ void tail_smooth(const TailLevel<T>& L, int mode, int degree, cg::clu
     tail_cheb_first_x(L, tid, nth);
     cl.sync();
   }
-  for (int k = 1; k < degree; ++k) {
+  for (int k = 1; k < L.degree; ++k) {
     tail_apply(L, L.d, L.t, tid, nth);
     cl.sync();
     tail_cheb_step(L, L.cheb + 2 * k, tid, nth);
@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(kTailThreads) k_vcycle_tail(const TailArgs<T> 
   // down: pre-smoothing, residual, restriction (+ the coarse first step)
   for (int l = 0; l < last; ++l) {
     const TailLevel<T>& L = a.L[l];
-    tail_smooth(L, (l > 0 || a.first_done) ? 1 : 0, a.degree, cl, tid, nth);
+    tail_smooth(L, (l > 0 || a.first_done) ? 1 : 0, cl, tid, nth);
     tail_apply(L, L.d, L.t, tid, nth);
     cl.sync();
     const bool first = !(l + 1 == last && a.inv);
@@ -260,18 +260,18 @@ __global__ void __launch_bounds__(kTailThreads) k_vcycle_tail(const TailArgs<T> 
     tail_dense(Lc, a.inv, a.ninv, tid, nth);
     cl.sync();
   } else {
-    tail_smooth(Lc, (last > 0 || a.first_done) ? 1 : 0, a.degree, cl, tid, nth);
+    tail_smooth(Lc, (last > 0 || a.first_done) ? 1 : 0, cl, tid, nth);
     for (int s = 1; s < a.coarse_sweeps; ++s) {
       tail_zero(Lc.r, 2 * Lc.nnod, tid, nth);
       cl.sync();
-      tail_smooth(Lc, 2, a.degree, cl, tid, nth);
+      tail_smooth(Lc, 2, cl, tid, nth);
     }
   }
   // up: prolongation and post-smoothing
   for (int l = last - 1; l >= 0; --l) {
     tail_prolong(a.L[l], a.L[l + 1], tid, nth);
     cl.sync();
-    tail_smooth(a.L[l], 2, a.degree, cl, tid, nth);
+    tail_smooth(a.L[l], 2, cl, tid, nth);
   }
 }
 
@@ -335,7 +335,6 @@ void launch_vcycle_tail(Ctx& c, size_t l0, const T* b, T* x, bool first_done, co
   TailArgs<T> a;
   std::memset(&a, 0, sizeof(a));
   a.nlev = (int)(c.mg.size() - l0);
-  a.degree = c.mg_degree;
   a.first_done = first_done ? 1 : 0;
   a.coarse_sweeps = o.coarse_sweeps;
   a.inv = c.coarse_n > 0 ? c.coarse_inv + (size_t)c.coarse_n * c.coarse_n : nullptr;
@@ -348,6 +347,7 @@ void launch_vcycle_tail(Ctx& c, size_t l0, const T* b, T* x, bool first_done, co
     L.cheb = M.cheb;
     L.x = (T*)M.x; L.b = (T*)M.b; L.r = (T*)M.r; L.d = (T*)M.d; L.t = (T*)M.t;
     L.ncr = M.g.ncr; L.nct = M.g.nct; L.pin = M.g.pin;
+    L.degree = M.degree;
     L.nel = (int)M.g.nel; L.nnod = (int)M.g.nnod; L.A = (int)M.g.A(); L.B = (int)M.g.B();
   }
   // the top level's b and x are the caller's vectors

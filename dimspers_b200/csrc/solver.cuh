@@ -23,6 +23,8 @@ struct SolveCfg {
   int schur_pc = 0;         // 0 lumped mass (StokesPcCG), 1 element-block mass inverse
   int launch_overlap = 1;   // 1: programmatic dependent launch between solver kernels
   int matrix_free = 0;      // 1: fine-level applies from the rotated tensors (no element matrices)
+  int true_residual = 1;    // 1: outer loop restarted until the true Schur residual meets rtol
+  int max_restarts = 4;
   MGOptions mg;
 };
 
@@ -46,6 +48,7 @@ struct SolveResult {
   int64_t refinements = 0;    // FP64 refinement steps (FP32-refined path)
   int fallback = 0;           // learned guess rejected
   double r0_guess = 0.0;      // ||r(P0)|| of the guess
+  int restarts = 0;           // passes of the outer loop in the true-residual mode
   double relres = 0.0, r0 = 0.0, omega = 0.0, div_residual = 0.0, mom_residual = 0.0;
 };
 

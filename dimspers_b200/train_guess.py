@@ -41,7 +41,7 @@ def main():
     mesh = build_mesh(args.nr, args.nt, "discontinuous")
     nrg, ntg = learned.grid_shape(args.nr, args.nt)
     ctx = StokesContext(args.nr, args.nt, "discontinuous")
-    solve_opts = dict(precision=1, schur_pc=1, inner_relax=1e-4, itmax=20000, raise_on_status=False)
+    solve_opts = dict(precision=1, schur_pc=1, inner_relax=1e-2, itmax=20000, raise_on_status=False)
     n = args.train + args.test
     X = torch.empty((n, 4, nrg, ntg), dtype=torch.float32, device=dev)
     Y = torch.empty((n, 1, nrg, ntg), dtype=torch.float32, device=dev)

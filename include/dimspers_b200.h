@@ -110,6 +110,14 @@ typedef struct {
                               element read instead of 312; slower on B200, where
                               the packed apply runs near HBM peak), 0 = packed
                               element matrices (default)                      */
+  int32_t cheb_degree_coarse; /* Chebyshev degree on the levels below the
+                              finest (0 = cheb_degree)                        */
+  int32_t true_residual;   /* 1 (default): when the outer loop stops, U is
+                              solved afresh, U = K^-1 (F + G P), and the loop
+                              restarts from P until the TRUE residual
+                              ||G^T U|| meets rtol (needed with inner_relax,
+                              where the recursive residual drifts); 0: stop on
+                              the recursive residual as StokesPcCG does      */
 } dp_solve_opts;
 
 typedef struct {
@@ -128,6 +136,7 @@ typedef struct {
   int64_t refinements;         /* FP64 refinement steps (FP32-refined path)   */
   double r0_guess;             /* use_guess = 2: ||r(P0)|| of the guess; r0 is then
                                   the zero-guess residual                     */
+  int32_t restarts;            /* passes of the outer loop (true_residual = 1)  */
 } dp_solve_report;
 
 typedef struct dp_ctx dp_ctx;

@@ -225,3 +225,23 @@ def test_matrix_free_apply_matches_packed_matrices(pressure, kind):
         assert r["status"] == 0
     for U, P, _, r in out[1:]:
         assert rel(U, out[0][0]) < 1e-7 and rel(P, out[0][1]) < 1e-7
+
+
+def test_true_residual_restart_with_relaxed_inner_solves():
+    """Loose inner solves (inner_relax = 1e-2): the outer loop is restarted
+    until the TRUE Schur residual meets rtol, and U = K^-1 (F + G P) holds to
+    the tight inner tolerance at the end."""
+    prob, mat, ctx = _setup(16, 128, "discontinuous", "aniso")
+    with ctx:
+        ctx.set_material(mat.eta_ip, mat.rho, mat.g, mat.C6)
+        ctx.assemble(1)
+        common = dict(want_cart=False, precision=1, schur_pc=1, rtol=1e-8, itmax=5000)
+        _, _, _, r1 = ctx.solve(inner_relax=1e-2, true_residual=1, **common)
+        _, _, _, r0 = ctx.solve(inner_relax=1e-2, true_residual=0, **common)
+        Ut, Pt, _, rt = ctx.solve(want_cart=False, precision=1, schur_pc=1, rtol=1e-11, inner_rtol=1e-12, itmax=5000)
+        U1, P1, _, _ = ctx.solve(inner_relax=1e-2, true_residual=1, **common)
+    assert r1["status"] == 0 and r1["restarts"] >= 1
+    assert r1["div_residual"] < 1e-8          # the true residual, not the recursive one
+    assert r1["mom_residual"] < 1e-8          # U solves the momentum equation for the final P
+    assert r0["mom_residual"] > 10 * r1["mom_residual"]
+    assert rel(U1, Ut) < 1e-4 and rel(P1, Pt) < 1e-2   # a 1e-8 solution of this P2-P1disc problem
