@@ -3,13 +3,16 @@
 // StokesPcCG (IterativeSolvers.jl:94-168) is a loop of outer Schur iterations,
 // each with an inner K-solve that is itself a loop (PCG, and for the
 // FP32-refined path a refinement loop around an FP32 PCG).  Every loop here
-// is a WHILE conditional graph node whose condition is set on the device by a
-// one-thread "check" kernel at the end of the body (cudaGraphSetConditional),
-// so a solve is one graph launch and one final synchronisation: no host
+// is a WHILE conditional graph node whose condition is set on the device
+// (cudaGraphSetConditional) at the end of its body, by a one-thread check
+// kernel or, for the inner PCG, by the last block of the update kernel, so a
+// solve is one graph launch and one final synchronisation: no host
 // round-trip per iteration.  Stopping tests are the reference's:
 //   outer: ||r|| < rtol * ||r0|| and it >= itmin, or it == itmax,
 //          or breakdown (q.Sq <= 0 / non-finite) -> status
 //   inner: ||y - K z|| <= inner_rtol ||y|| or inner_itmax.
+// In the true-residual mode the outer loop sits in one more WHILE loop that
+// re-solves U = K^-1 (F + G P) and restarts until the TRUE residual passes.
 // The captured sequence depends only on the hierarchy shape and the options
 // baked into it (precision, preconditioner, guess, rotation removal), so the
 // instantiated graph is cached in the context and reused across assemblies;
