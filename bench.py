@@ -72,7 +72,7 @@ def parse():
 
 
 # solver options of the two arms
-FAST = dict(precision=1, cheb_degree=3, cheb_lo=0.05, inner_rtol=1e-10, inner_relax=1e-2, schur_pc=1)
+FAST = dict(precision=1, cheb_degree=3, cheb_lo=0.05, inner_rtol=1e-10, inner_relax=1e-2, relax_base=1e-8, schur_pc=1)
 PLAIN = dict(precision=0, cheb_degree=3, cheb_lo=0.05, inner_rtol=1e-10, inner_relax=0.0, schur_pc=0)
 
 

@@ -33,7 +33,8 @@ class SolveOpts(C.Structure):
                 ("coarse_max", C.c_int32), ("schur_pc", C.c_int32),
                 ("apply_warps", C.c_int32), ("apply_warps_t", C.c_int32),
                 ("launch_overlap", C.c_int32), ("mg_tail", C.c_int32),
-                ("matrix_free", C.c_int32), ("cheb_degree_coarse", C.c_int32), ("true_residual", C.c_int32)]
+                ("matrix_free", C.c_int32), ("cheb_degree_coarse", C.c_int32), ("true_residual", C.c_int32),
+                ("relax_base", C.c_double)]
 
 
 class SolveReport(C.Structure):

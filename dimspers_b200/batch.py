@@ -38,7 +38,7 @@ from ._lib import DP_MEM_DEVICE, DP_MEM_HOST, SolveOpts, SolveReport, check, lib
 from .stokes import StokesContext, default_opts
 
 SIZES = ((32, 256), (64, 512), (128, 1024), (256, 2048))
-FAST = dict(precision=1, cheb_degree=3, cheb_lo=0.05, inner_rtol=1e-10, inner_relax=1e-2, schur_pc=1)
+FAST = dict(precision=1, cheb_degree=3, cheb_lo=0.05, inner_rtol=1e-10, inner_relax=1e-2, relax_base=1e-8, schur_pc=1)
 TUNE_SPACE = dict(apply=((4, 1), (8, 1), (4, 4), (8, 2)), cheb_degree=(2, 3, 4), coarse_max=(1024, 1536))
 
 

@@ -131,6 +131,8 @@ static SolveCfg make_cfg(const dp_solve_opts* o) {
   cfg.matrix_free = o->matrix_free;
   if (o->true_residual != 0 && o->true_residual != 1) throw BadArg("true_residual must be 0 or 1");
   cfg.true_residual = o->true_residual;
+  if (!(o->relax_base >= 0.0) || o->relax_base >= 1.0) throw BadArg("relax_base must be in [0, 1)");
+  cfg.relax_base = o->relax_base;
   if (o->mg_tail < 0) throw BadArg("mg_tail must be 0 (off) or a positive element count");
   cfg.mg.tail_max_el = o->mg_tail;
   if (o->apply_warps > 0) cfg.mg.apply_warps = o->apply_warps;
@@ -378,6 +380,7 @@ void dp_default_opts(dp_solve_opts* o) {
   o->mg_tail = 0;
   o->matrix_free = 0;
   o->true_residual = 1;
+  o->relax_base = 0.0;
 }
 
 const char* dp_status_string(int s) {

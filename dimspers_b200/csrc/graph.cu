@@ -30,7 +30,7 @@ namespace dp {
 
 struct DevCtl {
   // parameters (written by the host before each launch)
-  double rtol, inner_rtol, inner_rtol32, relax_cap;
+  double rtol, inner_rtol, inner_rtol32, relax_cap, relax_base;
   int itmax, itmin, inner_itmax, max_refine;
   // state
   int outer_it, in_it, in32_it, ref_it, status, guess_used, restarts, max_restarts;
@@ -44,13 +44,15 @@ enum GSlot { G_RZ = 16, G_RZN = 17, G_PAP = 18, G_IRR = 19, G_YY = 20,
 
 // ---- control kernels (one thread) ---------------------------------------------
 // Inner tolerance: fixed, or (relax) loosened in proportion to the outer
-// residual, rtol_k = min(cap, inner_rtol * ||r0|| / ||r_k||): an inexact-Krylov
-// relaxation that keeps the product of step size and inner error bounded.
+// residual, rtol_k = min(cap, max(inner_rtol, base * ||r0|| / ||r_k||)): an
+// inexact-Krylov relaxation that keeps the product of step size and inner
+// error bounded (base: the outer target's scale; inner_rtol when unset).
 __device__ inline double inner_rtol_now(const DevCtl* ctl, const double* scal, int relax) {
   double rt = ctl->inner_rtol;
   if (relax && ctl->relax_cap > 0.0 && ctl->r0 > 0.0) {
     const double rk = sqrt(scal[S_RR]);
-    if (rk > 0.0) rt = fmin(ctl->relax_cap, fmax(rt, rt * ctl->r0 / rk));
+    const double base = ctl->relax_base > 0.0 ? ctl->relax_base : ctl->inner_rtol;
+    if (rk > 0.0) rt = fmin(ctl->relax_cap, fmax(rt, base * ctl->r0 / rk));
   }
   return rt;
 }
@@ -592,6 +594,7 @@ static void upload_params(Ctx& c, const SolveCfg& cfg, cudaStream_t s) {
   h.inner_rtol = cfg.inner_rtol;
   h.inner_rtol32 = cfg.inner_rtol32;
   h.relax_cap = cfg.inner_relax;
+  h.relax_base = cfg.relax_base;
   h.itmax = cfg.itmax;
   h.itmin = cfg.itmin;
   h.inner_itmax = cfg.inner_itmax;

@@ -20,6 +20,7 @@ struct SolveCfg {
   int verbose = 0;
   int host_loop = 0;        // 1: host-driven loops (debug); 0: one CUDA graph per solve
   double inner_relax = 0.0; // > 0: relaxed inner tolerance with this cap
+  double relax_base = 0.0;  // base of the relaxation (0: inner_rtol)
   int schur_pc = 0;         // 0 lumped mass (StokesPcCG), 1 element-block mass inverse
   int launch_overlap = 1;   // 1: programmatic dependent launch between solver kernels
   int matrix_free = 0;      // 1: fine-level applies from the rotated tensors (no element matrices)

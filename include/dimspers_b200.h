@@ -118,6 +118,11 @@ typedef struct {
                               ||G^T U|| meets rtol (needed with inner_relax,
                               where the recursive residual drifts); 0: stop on
                               the recursive residual as StokesPcCG does      */
+  double relax_base;       /* with inner_relax > 0: inner tolerance of outer
+                              iteration k = min(inner_relax, max(inner_rtol,
+                              relax_base * ||r0|| / ||r_k||)); 0 = inner_rtol.
+                              The initial and true-residual solves keep
+                              inner_rtol.                                     */
 } dp_solve_opts;
 
 typedef struct {
