@@ -85,3 +85,41 @@ def test_sizes_match_survey_table():
         assert _lib.lib().dp_mesh_sizes(C.byref(d), C.byref(a), C.byref(b), C.byref(c_), C.byref(f)) == 0
         assert (a.value, b.value, c_.value) == (nel, nnod, npd)
         assert f.value == 2 * 2 * nct + 1
+
+
+def _header_struct_fields(name):
+    """Field names of a typedef struct { ... } name; in the C header, in order."""
+    hdr = open(os.path.join(ROOT, "include", "dimspers_b200.h")).read()
+    end = hdr.index("} " + name + ";")
+    start = hdr.rindex("typedef struct {", 0, end) + len("typedef struct {")
+    body = hdr[start:end]
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    fields = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        typ, names = decl.split(None, 1)
+        fields += [n.strip() for n in names.split(",")]
+    return fields
+
+
+@pytest.mark.parametrize("cname,pystruct", [("dp_solve_opts", "SolveOpts"), ("dp_solve_report", "SolveReport"),
+                                            ("dp_mesh_desc", "MeshDesc")])
+def test_ctypes_structs_mirror_the_header(cname, pystruct):
+    """The ctypes mirrors list the header's fields in the header's order."""
+    py = [f for f, _ in getattr(_lib, pystruct)._fields_]
+    assert py == _header_struct_fields(cname)
+
+
+def test_default_opts_fill_exactly_the_struct():
+    """dp_default_opts writes the whole options struct and nothing beyond it
+    (a shorter mirror would let the library write past the caller's buffer)."""
+    import ctypes as C
+    n = C.sizeof(_lib.SolveOpts)
+    buf = (C.c_ubyte * (n + 64))(*([0xAB] * (n + 64)))
+    _lib.lib().dp_default_opts(C.cast(buf, C.POINTER(_lib.SolveOpts)))
+    assert bytes(buf[n:]) == bytes([0xAB] * 64)
+    o = _lib.SolveOpts.from_buffer(buf)
+    assert (o.rtol, o.itmax, o.itmin, o.cheb_degree, o.coarse_max) == (1e-8, 200, 10, 3, 1536)
+    assert (o.launch_overlap, o.true_residual, o.matrix_free, o.mg_tail, o.relax_base) == (1, 1, 0, 0, 0.0)
