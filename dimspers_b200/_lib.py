@@ -78,6 +78,7 @@ SIGNATURES = {
     "dp_get_rhs": (C.c_int, [_P, _P, _P]),
     "dp_default_opts": (None, [C.POINTER(SolveOpts)]),
     "dp_profile_kernel": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
+    "dp_stress": (C.c_int, [_P, _P, _P, C.c_int64, C.POINTER(_P), C.c_int64, _P, C.c_int32]),
     "dp_batch_create": (C.c_int, [C.POINTER(_P), C.c_int32, _P, C.POINTER(_P)]),
     "dp_batch_run": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.c_int32, _P,
                                C.POINTER(C.c_double)]),

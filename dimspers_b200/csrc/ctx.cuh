@@ -113,6 +113,8 @@ struct Ctx {
   double* Minv = nullptr;       // 6*nel inverse element mass blocks (discontinuous pressure)
   double* Fscale = nullptr;
   void* flush = nullptr;        // L2 flush buffer for cold kernel timings
+  double* stress_buf = nullptr; // post-processor staging: eta 7, tensor 42, outputs 56 per element
+  bool stress_tensor = false;   // the staged inputs carry a tensor
 
   // multigrid hierarchy (level 0 = fine)
   std::vector<MGLevel> mg;

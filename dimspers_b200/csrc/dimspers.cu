@@ -8,5 +8,6 @@
 #include "solver.cu"
 #include "graph.cu"
 #include "capi.cu"
+#include "stress.cu"
 #include "noalloc.cu"
 #include "cnn.cu"

@@ -212,6 +212,27 @@ class StokesContext:
         self._chk(lib().dp_apply_GT(self.h, _ptr(x), _ptr(p), DP_MEM_HOST))
         return p
 
+    def stress(self, Ucart, eta_ip, C6=None):
+        """stress! (src/Stress/StressCalculation.jl:244-249) for the Cartesian
+        velocity Ucart (2*nnod, reference numbering): dict of (nel, 7) arrays
+        exx, ezz, exz, eII, txx, tzz, txz, tII at the 7-point IPs."""
+        U = np.ascontiguousarray(Ucart, dtype=np.float64)
+        eta = np.asfortranarray(eta_ip, dtype=np.float64)
+        if eta.shape[1] < 7:
+            raise ValueError("eta_ip needs 7 IP columns")
+        fields, keep, ldc = None, [], 0
+        if C6 is not None:
+            keep = [np.asfortranarray(f, dtype=np.float64) for f in C6]
+            fields = (C.c_void_p * 6)(*[f.ctypes.data for f in keep])
+            ldc = keep[0].shape[0]
+        out = np.empty(8 * 7 * self.nel)
+        self._chk(lib().dp_stress(self.h, _ptr(U), _ptr(eta), eta.shape[0],
+                                  C.cast(fields, C.POINTER(C.c_void_p)) if fields is not None else None, ldc,
+                                  _ptr(out), DP_MEM_HOST))
+        names = ("exx", "ezz", "exz", "eII", "txx", "tzz", "txz", "tII")
+        blocks = out.reshape(8, 7, self.nel)
+        return {n: blocks[i].T.copy() for i, n in enumerate(names)}
+
     def rhs(self):
         F = np.empty(2 * self.nnod)
         pc = np.empty(self.npres)

@@ -234,6 +234,18 @@ void dp_default_opts(dp_solve_opts* opts);
  * on a device looks up the array's address; make it before any stream capture. */
 int dp_apply_K_noalloc(dp_ctx* ctx, const double* x, double* y);
 
+/* ---- strain-rate / stress post-processor --------------------------------
+ * stress! (src/Stress/StressCalculation.jl:23-249; MAIN.jl:241-243): per
+ * element and 7-point IP (Quadrature.jl:109-138), the strain rate of the
+ * Cartesian velocity Ucart (interleaved [ux, uz], reference numbering), its
+ * second invariant, the deviatoric stress (isotropic eta, or the tensor fields
+ * C6 in StiffnessTensor order with the reference's anisotropic formula) and
+ * its second invariant.  eta_ip and the C6 fields: nel x ld element-fastest
+ * (columns 1..7 read).  out: 8 matrices nel x 7 (element fastest), in the
+ * order eps.xx, eps.zz, eps.xz, epsII, tau.xx, tau.zz, tau.xz, tauII. */
+int dp_stress(dp_ctx* ctx, const double* Ucart, const double* eta_ip, int64_t ld_eta,
+              const double* const* C6, int64_t ld_C, double* out, int32_t mem);
+
 /* ---- batches of independent solves ---------------------------------------
  * Independent problems (contexts of any resolution, all on one device) solved
  * by ONE graph launch: the batch graph holds one branch per context with that
@@ -277,7 +289,8 @@ int dp_guess_from_grid(dp_ctx* ctx, const float* p_grid, int32_t nrg, int32_t nt
 /* Average device time (ms) of one launch of a hot kernel on the context's
  * stream, from CUDA events, after an assembly: which = 0 fine-level A-apply
  * FP32, 1 fine-level A-apply FP64, 2 one multigrid V-cycle (precision of the
- * last solve).  flush_l2 = 0: `reps` back-to-back launches (warm L2);
+ * last solve), 3 the stress post-processor on the inputs of the last
+ * dp_stress call.  flush_l2 = 0: `reps` back-to-back launches (warm L2);
  * 1: a 256 MB buffer is read before each launch and each launch is timed
  * alone (cold L2, DRAM-bound figure). */
 int dp_profile_kernel(dp_ctx* ctx, int32_t which, int32_t reps, int32_t flush_l2, double* ms_per_launch);

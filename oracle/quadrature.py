@@ -7,6 +7,7 @@ Follows src/Algebra/Quadrature.jl:
   sf_dN_tri6        :287-307
   sf_N_tri3/dN_tri3 :166-199  (linear N3 and P1 pressure NP)
   _get_SF           :35-49
+  ip_triangle7      :109-138  (the stress post-processor's rule, centroid first)
 """
 import numpy as np
 
@@ -26,6 +27,25 @@ def ip_triangle6():
     w1 = (620.0 + np.sqrt(213125.0 - 53320.0 * np.sqrt(10.0))) / 3720.0
     w2 = (620.0 - np.sqrt(213125.0 - 53320.0 * np.sqrt(10.0))) / 3720.0
     ipw = np.array([w1, w1, w1, w2, w2, w2])
+    return ipx, 0.5 * ipw
+
+
+def ip_triangle7():
+    """7-point rule (7x2: r, s) and weights -- Quadrature.jl:109-138."""
+    g1 = (6.0 - np.sqrt(15.0)) / 21.0
+    g2 = (6.0 + np.sqrt(15.0)) / 21.0
+    ipx = np.array([
+        [1.0 / 3.0, 1.0 / 3.0],
+        [1.0 - 2.0 * g1, g1],
+        [g1, 1.0 - 2.0 * g1],
+        [g1, g1],
+        [1.0 - 2.0 * g2, g2],
+        [g2, 1.0 - 2.0 * g2],
+        [g2, g2],
+    ])
+    w1 = (155.0 - np.sqrt(15.0)) / 1200.0
+    w2 = (155.0 + np.sqrt(15.0)) / 1200.0
+    ipw = np.array([0.225, w1, w1, w1, w2, w2, w2])
     return ipx, 0.5 * ipw
 
 

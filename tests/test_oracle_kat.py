@@ -128,3 +128,31 @@ def test_oracle_reproduces_golden(name):
     assert rel(out["mats"]["F"], gold["F"]) < 1e-14
     import hashlib
     assert hashlib.sha256(np.ascontiguousarray(prob.gr.e2n).tobytes()).hexdigest() == meta["e2n_sha256"]
+
+
+def test_stress_rigid_rotation_and_linear_fields_converge_second_order():
+    """The post-processor's strain rate of a rigid rotation is 0 and that of a
+    linear Cartesian field is its gradient, up to the O(h^2) error of
+    interpolating it on (theta, r)-linear elements: the error falls 4x per
+    refinement."""
+    import oracle.stress as ST
+    errs = []
+    for n in (4, 8, 16):
+        prob = OS.make_problem(n, 8 * n, "discontinuous")
+        th, r, e2n = prob.th, prob.r, prob.gr.e2n
+        x, z = prob.gr.r * np.sin(prob.gr.theta), prob.gr.r * np.cos(prob.gr.theta)
+        one = np.ones((th.shape[1], 7))
+        U = np.zeros(2 * x.size)
+        U[0::2], U[1::2] = -z, x
+        o = ST.stress(U, one, th, r, e2n)
+        e_rot = max(np.abs(o[k]).max() for k in ("exx", "ezz", "exz"))
+        U[0::2], U[1::2] = 2 * x, -3 * z
+        o = ST.stress(U, one, th, r, e2n)
+        e_lin = max(np.abs(o["exx"] - 2).max(), np.abs(o["ezz"] + 3).max(), np.abs(o["exz"]).max())
+        errs.append((e_rot, e_lin))
+    for (a0, b0), (a1, b1) in zip(errs, errs[1:]):
+        assert 3.5 < a0 / a1 < 4.5 and 3.5 < b0 / b1 < 4.5
+    # invariants and the isotropic stress of the linear field (eta = 1)
+    assert np.allclose(o["eII"], np.sqrt(0.5 * (o["exx"] ** 2 + o["ezz"] ** 2) + o["exz"] ** 2))
+    assert np.allclose(o["txx"], 4 / 3 * o["exx"] - 2 / 3 * o["ezz"])
+    assert np.allclose(o["txz"], 2 * o["exz"])
