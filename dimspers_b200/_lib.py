@@ -37,6 +37,11 @@ class SolveOpts(C.Structure):
                 ("relax_base", C.c_double)]
 
 
+class Arrhenius(C.Structure):
+    _fields_ = [("eta0", C.c_double), ("R", C.c_double), ("Ea", C.c_double), ("Va", C.c_double),
+                ("T0", C.c_double), ("phi_deg", C.c_double)]
+
+
 class SolveReport(C.Structure):
     _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("inner_iterations", C.c_int64),
                 ("relres", C.c_double), ("r0", C.c_double), ("omega", C.c_double),
@@ -79,6 +84,7 @@ SIGNATURES = {
     "dp_default_opts": (None, [C.POINTER(SolveOpts)]),
     "dp_profile_kernel": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     "dp_stress": (C.c_int, [_P, _P, _P, C.c_int64, C.POINTER(_P), C.c_int64, _P, C.c_int32]),
+    "dp_viscosity_arrhenius": (C.c_int, [_P, C.POINTER(Arrhenius), _P, _P, C.c_int64, _P, _P, _P, _P, _P, C.c_int32]),
     "dp_batch_create": (C.c_int, [C.POINTER(_P), C.c_int32, _P, C.POINTER(_P)]),
     "dp_batch_run": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.c_int32, _P,
                                C.POINTER(C.c_double)]),

@@ -33,6 +33,7 @@ Ctx::~Ctx() {
   cudaFree(K64); cudaFree(K32); cudaFree(Gp); cudaFree(F); cudaFree(pc); cudaFree(Minv); cudaFree(Fscale);
   cudaFree(flush);
   cudaFree(stress_buf);
+  cudaFree(rheo_buf);
   cudaFree(scal); cudaFreeHost(h_scal); cudaFree(partial); cudaFree(counter);
   for (void* p : work) cudaFree(p);
   if (stream) cudaStreamDestroy(stream);
@@ -751,6 +752,7 @@ __global__ void k_flush_read(const uint4* __restrict__ buf, int64_t n, unsigned 
 
 namespace dp {
 void launch_stress_staged(Ctx& c, bool tensor);
+void launch_viscosity_staged(Ctx& c);
 }
 
 int dp_profile_kernel(dp_ctx* h, int32_t which, int32_t reps, int32_t flush_l2, double* ms) {
@@ -758,12 +760,13 @@ int dp_profile_kernel(dp_ctx* h, int32_t which, int32_t reps, int32_t flush_l2, 
   Ctx& c = h->c;
   return guarded(&c, [&] {
     DP_CUDA(cudaSetDevice(c.device));
-    if (which != 3 && c.assembled < 0) throw BadArg("dp_assemble must run first");
+    if (which < 3 && c.assembled < 0) throw BadArg("dp_assemble must run first");
     if (reps < 1 || !ms) throw BadArg("reps must be >= 1");
     if (which == 0 && !c.K32) throw BadArg("no FP32 element matrices (assemble with precision 1)");
     if (which == 2 && c.mg.empty()) throw BadArg("no multigrid hierarchy (run a solve first)");
     if (which == 3 && !c.stress_buf) throw BadArg("no staged post-processor inputs (call dp_stress first)");
-    if (which < 0 || which > 3) throw BadArg("which must be 0..3");
+    if (which == 4 && !c.rheo_buf) throw BadArg("no staged viscosity inputs (call dp_viscosity_arrhenius first)");
+    if (which < 0 || which > 4) throw BadArg("which must be 0..4");
     const int64_t n = 2 * c.fine.nnod;
     double* x64 = (double*)c.work[W_IN_P];
     double* y64 = (double*)c.work[W_IN_AP];
@@ -779,6 +782,7 @@ int dp_profile_kernel(dp_ctx* h, int32_t which, int32_t reps, int32_t flush_l2, 
       if (which == 0) launch_apply_K_acc<float, float>(c.fine, c.K32, x32, y32, c.stream);
       else if (which == 1) launch_apply_K_acc<double, double>(c.fine, c.K64, x64, y64, c.stream);
       else if (which == 3) launch_stress_staged(c, c.stress_tensor);
+      else if (which == 4) launch_viscosity_staged(c);
       else if (c.mg_prec == 1) mg_apply_f(c, x32, y32, MGOptions());
       else mg_apply(c, x64, y64, MGOptions());
     };

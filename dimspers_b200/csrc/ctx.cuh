@@ -115,6 +115,8 @@ struct Ctx {
   void* flush = nullptr;        // L2 flush buffer for cold kernel timings
   double* stress_buf = nullptr; // post-processor staging: eta 7, tensor 42, outputs 56 per element
   bool stress_tensor = false;   // the staged inputs carry a tensor
+  double* rheo_buf = nullptr;   // viscosity update staging: 4 x 7 per element, 4 per node
+  double rheo_law[8] = {};      // the last viscosity update's law (eta0, R, Ea, Va, T0, sin, cos, phi)
 
   // multigrid hierarchy (level 0 = fine)
   std::vector<MGLevel> mg;

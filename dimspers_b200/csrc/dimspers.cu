@@ -9,5 +9,6 @@
 #include "graph.cu"
 #include "capi.cu"
 #include "stress.cu"
+#include "rheology.cu"
 #include "noalloc.cu"
 #include "cnn.cu"

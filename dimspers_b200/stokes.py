@@ -233,6 +233,23 @@ class StokesContext:
         blocks = out.reshape(8, 7, self.nel)
         return {n: blocks[i].T.copy() for i, n in enumerate(names)}
 
+    def viscosity_arrhenius(self, eta_ip, T, P_vertex, r, epsII, tauII, cohesion, eta0=5e20, R=8.314, Ea=100e3,
+                            Va=1e-6, T0=1600.0, phi=1.0):
+        """getviscosity!(::Arrhenius, ...) (src/Rheology/Rheology.jl:348-403):
+        the updated (nel, 7) eta.ip from nodal T and r (reference numbering),
+        vertex pressure, and the (nel, 7) epsII, tauII and cohesion."""
+        law = _lib.Arrhenius(eta0, R, Ea, Va, T0, phi)
+        eta = np.asfortranarray(eta_ip, dtype=np.float64).copy(order="F")
+        mats = [np.asfortranarray(a, dtype=np.float64) for a in (epsII, tauII, cohesion)]
+        for a in [eta] + mats:
+            if a.shape != (self.nel, 7):
+                raise ValueError("IP arrays must be (nel, 7)")
+        vec = [np.ascontiguousarray(a, dtype=np.float64) for a in (T, P_vertex, r)]
+        self._chk(lib().dp_viscosity_arrhenius(self.h, C.byref(law), _ptr(vec[0]), _ptr(vec[1]), vec[1].size,
+                                               _ptr(vec[2]), _ptr(mats[0]), _ptr(mats[1]), _ptr(mats[2]),
+                                               _ptr(eta), DP_MEM_HOST))
+        return np.array(eta)
+
     def rhs(self):
         F = np.empty(2 * self.nnod)
         pc = np.empty(self.npres)
@@ -265,7 +282,8 @@ class StokesContext:
         return rep.as_dict()
 
     def profile_kernel(self, which, reps=50, flush_l2=False):
-        """Average ms per launch: 0 FP32 A-apply, 1 FP64 A-apply, 2 V-cycle;
+        """Average ms per launch: 0 FP32 A-apply, 1 FP64 A-apply, 2 V-cycle,
+        3 stress post-processor, 4 viscosity update (last call's inputs);
         flush_l2 times each launch alone after overwriting 256 MB (cold L2)."""
         ms = C.c_double(0.0)
         self._chk(lib().dp_profile_kernel(self.h, int(which), int(reps), 1 if flush_l2 else 0, C.byref(ms)))

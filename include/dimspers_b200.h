@@ -246,6 +246,22 @@ int dp_apply_K_noalloc(dp_ctx* ctx, const double* x, double* y);
 int dp_stress(dp_ctx* ctx, const double* Ucart, const double* eta_ip, int64_t ld_eta,
               const double* const* C6, int64_t ld_C, double* out, int32_t mem);
 
+/* ---- per-IP viscosity update (Arrhenius law, Drucker-Prager plasticity) --
+ * getviscosity!(::Arrhenius, ...) (src/Rheology/Rheology.jl:348-403; law
+ * :60-97, :171-173): at the 7-point IPs, eta = clamp(lambda(z) eta0 exp((Ea +
+ * P Va)/(R T) - Ea/(R T0)), 1e18, 1e25) with T and z = r by P2 interpolation
+ * and P by linear interpolation of the vertex pressure plus |min P|; where
+ * cohesion, phi and epsII are non-zero, eta = clamp(tau_y / (2 epsII), 1e18,
+ * 1e25) if tau_y = cosd(phi) C + sind(phi) P < tauII, else unchanged.
+ * T_node, r_node: nnod (reference numbering); P_vertex: the nvert vertex
+ * values; epsII, tauII, cohesion, eta_ip (in/out): nel x 7 element-fastest. */
+typedef struct {
+  double eta0, R, Ea, Va, T0, phi_deg;
+} dp_arrhenius;
+int dp_viscosity_arrhenius(dp_ctx* ctx, const dp_arrhenius* law, const double* T_node, const double* P_vertex,
+                           int64_t nvert, const double* r_node, const double* epsII, const double* tauII,
+                           const double* cohesion, double* eta_ip, int32_t mem);
+
 /* ---- batches of independent solves ---------------------------------------
  * Independent problems (contexts of any resolution, all on one device) solved
  * by ONE graph launch: the batch graph holds one branch per context with that
@@ -290,7 +306,8 @@ int dp_guess_from_grid(dp_ctx* ctx, const float* p_grid, int32_t nrg, int32_t nt
  * stream, from CUDA events, after an assembly: which = 0 fine-level A-apply
  * FP32, 1 fine-level A-apply FP64, 2 one multigrid V-cycle (precision of the
  * last solve), 3 the stress post-processor on the inputs of the last
- * dp_stress call.  flush_l2 = 0: `reps` back-to-back launches (warm L2);
+ * dp_stress call, 4 the viscosity update on the inputs of the last
+ * dp_viscosity_arrhenius call.  flush_l2 = 0: `reps` back-to-back launches (warm L2);
  * 1: a 256 MB buffer is read before each launch and each launch is timed
  * alone (cold L2, DRAM-bound figure). */
 int dp_profile_kernel(dp_ctx* ctx, int32_t which, int32_t reps, int32_t flush_l2, double* ms_per_launch);

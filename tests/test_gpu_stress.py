@@ -47,3 +47,30 @@ def test_stress_of_a_solve_matches_oracle():
     for k in ST.NAMES:
         assert _max_rel(got[k], ref[k]) < 1e-12, k
     assert np.all(got["eII"] >= 0) and np.all(got["tII"] >= 0)
+
+
+def test_arrhenius_viscosity_update_matches_oracle():
+    """getviscosity!(::Arrhenius) on dimensional inputs: every branch (depth
+    zones, clamps, plastic yield, plastic-but-not-yielding kept, no cohesion)."""
+    from dimspers_b200 import StokesContext
+    import oracle.rheology as RH
+    prob = OS.make_problem(8, 64, "continuous")
+    nel, nn = prob.th.shape[1], prob.gr.r.size
+    nv = 9 * 64
+    rng = np.random.default_rng(11)
+    r = 3.48e6 + (prob.gr.r - 1.22) * 2.87e6           # radius in m: all three depth zones
+    T = 1300.0 + 1200.0 * rng.random(nn)
+    P = 2e9 * rng.standard_normal(nv)
+    eps = np.abs(rng.standard_normal((nel, 7))) * 1e-15
+    eps[::5] = 0.0                                     # no strain rate: the non-plastic branch
+    tau = 4e9 * rng.random((nel, 7))
+    coh = np.where(rng.random((nel, 7)) < 0.3, 0.0, 30e6)
+    eta0 = np.full((nel, 7), 3.3e21)
+    law = dict(eta0=5e20, R=8.314, Ea=100e3, Va=1e-6, T0=1600.0, phi=30.0)
+    ref = RH.arrhenius_viscosity(eta0, T, P, r, prob.gr.e2n, eps, tau, coh, law["eta0"], law["R"], law["Ea"],
+                                 law["Va"], law["T0"], law["phi"])
+    with StokesContext(8, 64, "continuous") as ctx:
+        got = ctx.viscosity_arrhenius(eta0, T, P, r, eps, tau, coh, **law)
+    assert np.abs(got / ref - 1).max() < 1e-12
+    kept = ref == 3.3e21
+    assert kept.any() and (ref == 1e18).any() and (~kept & (ref > 1e18)).any()

@@ -156,3 +156,49 @@ def test_stress_rigid_rotation_and_linear_fields_converge_second_order():
     assert np.allclose(o["eII"], np.sqrt(0.5 * (o["exx"] ** 2 + o["ezz"] ** 2) + o["exz"] ** 2))
     assert np.allclose(o["txx"], 4 / 3 * o["exx"] - 2 / 3 * o["ezz"])
     assert np.allclose(o["txz"], 2 * o["exz"])
+
+
+def test_arrhenius_update_branches_scalar_restatement():
+    """The vectorised viscosity update against a scalar per-IP loop written
+    straight from getviscosity!(::Arrhenius) (Rheology.jl:348-403) on a few
+    elements, with every branch present."""
+    from oracle import rheology as RH
+    prob = OS.make_problem(4, 16, "continuous")
+    e2n, nel = prob.gr.e2n, prob.gr.e2n.shape[1]
+    rng = np.random.default_rng(2)
+    r = 3.48e6 + (prob.gr.r - 1.22) * 2.87e6
+    T = 1300.0 + 1200.0 * rng.random(r.size)
+    P = 2e9 * rng.standard_normal(e2n[:3].max() + 1)
+    eps = np.abs(rng.standard_normal((nel, 7))) * 1e-15
+    eps[::4] = 0.0
+    tau = 4e9 * rng.random((nel, 7))
+    coh = np.where(rng.random((nel, 7)) < 0.3, 0.0, 30e6)
+    prev = np.full((nel, 7), 2e21)
+    law = (5e20, 8.314, 100e3, 1e-6, 1600.0, 30.0)
+    got = RH.arrhenius_viscosity(prev, T, P, r, e2n, eps, tau, coh, *law)
+    eta0, R, Ea, Va, T0, phi = law
+    ipx, _ = OQ.ip_triangle7()
+    minP, maxr = abs(P.min()), r.max()
+    branches = set()
+    for e in range(nel):
+        for ip in range(7):
+            a, b = ipx[ip]
+            c = 1.0 - a - b
+            N6 = [c * (2 * c - 1), a * (2 * a - 1), b * (2 * b - 1), 4 * a * c, 4 * a * b, 4 * b * c]
+            Tip = sum(N6[k] * T[e2n[k, e]] for k in range(6))
+            zip_ = sum(N6[k] * r[e2n[k, e]] for k in range(6))
+            Pip = c * P[e2n[0, e]] + a * P[e2n[1, e]] + b * P[e2n[2, e]] + minP
+            lam = 1e-3 if zip_ < maxr - 2780e3 else (1e0 if zip_ > maxr - 660e3 else 1e1)
+            want = min(max(lam * eta0 * math.exp((Ea + Pip * Va) / R / Tip - Ea / R / T0), 1e18), 1e25)
+            if coh[e, ip] != 0 and phi != 0 and eps[e, ip] != 0:
+                ty = math.cos(math.radians(phi)) * coh[e, ip] + math.sin(math.radians(phi)) * Pip
+                if ty < tau[e, ip]:
+                    want = max(1e18, min(1e25, ty / (2 * eps[e, ip])))
+                    branches.add("yield")
+                else:
+                    want = prev[e, ip]
+                    branches.add("kept")
+            else:
+                branches.add("creep")
+            assert math.isclose(got[e, ip], want, rel_tol=1e-13), (e, ip)
+    assert branches == {"yield", "kept", "creep"}
