@@ -42,6 +42,11 @@ class Arrhenius(C.Structure):
                 ("T0", C.c_double), ("phi_deg", C.c_double)]
 
 
+class Dem(C.Structure):
+    _fields_ = [("C", C.c_void_p), ("nrows", C.c_int64), ("a1a2_blk", C.c_void_p), ("n_a1a2", C.c_int64),
+                ("a2a3_blk", C.c_void_p), ("permutation_blk", C.c_void_p), ("sblk", C.c_int64), ("w", C.c_double)]
+
+
 class SolveReport(C.Structure):
     _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("inner_iterations", C.c_int64),
                 ("relres", C.c_double), ("r0", C.c_double), ("omega", C.c_double),
@@ -85,6 +90,9 @@ SIGNATURES = {
     "dp_profile_kernel": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     "dp_stress": (C.c_int, [_P, _P, _P, C.c_int64, C.POINTER(_P), C.c_int64, _P, C.c_int32]),
     "dp_viscosity_arrhenius": (C.c_int, [_P, C.POINTER(Arrhenius), _P, _P, C.c_int64, _P, _P, _P, _P, _P, C.c_int32]),
+    "dp_fse": (C.c_int, [_P, _P, C.POINTER(_P), C.c_int64, C.c_int32]),
+    "dp_anisotropic_tensor": (C.c_int, [_P, C.POINTER(Dem), _P, _P, _P, _P, C.c_int64, C.POINTER(_P), C.c_int64,
+                                        C.c_int32]),
     "dp_batch_create": (C.c_int, [C.POINTER(_P), C.c_int32, _P, C.POINTER(_P)]),
     "dp_batch_run": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.c_int32, _P,
                                C.POINTER(C.c_double)]),

@@ -465,23 +465,35 @@ void launch_ti_tensor_fill(Ctx& c, const double* delta, const double* dx, const 
   DP_LAUNCH_CHECK();
 }
 
-// Major eigenvector of L = F F^T per element (FSE.jl:143-161, eigval_order :189).
-// F per element in Julia 2x2 column-major order: F11, F21, F12, F22.
-__global__ void k_fse_director(int64_t nel, const double* F, double* dxo, double* dyo) {
-  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (e >= nel) return;
-  const double f11 = F[4 * e + 0], f21 = F[4 * e + 1], f12 = F[4 * e + 2], f22 = F[4 * e + 3];
+// Major eigenvector (vx, vy) and the eigenvalues of L = F F^T (FSE.jl:143-161,
+// eigval_order :189), F in Julia 2x2 column-major order F11, F21, F12, F22.
+// The eigenvector is taken from whichever row of L - lmax I is longer; a
+// multiple of the identity gives (1, 0).  lmin = det(L) / lmax (no
+// cancellation for elongated ellipsoids).
+__device__ __forceinline__ void fse_axes(double f11, double f21, double f12, double f22, double& vx, double& vy,
+                                         double& lmax, double& lmin) {
   const double l11 = f11 * f11 + f12 * f12;
   const double l12 = f11 * f21 + f12 * f22;
   const double l22 = f21 * f21 + f22 * f22;
   const double half_tr = 0.5 * (l11 + l22);
   const double disc = sqrt(0.25 * (l11 - l22) * (l11 - l22) + l12 * l12);
-  const double lmax = half_tr + disc;
+  lmax = half_tr + disc;
   const double ax = l12, ay = lmax - l11, bx = lmax - l22, by = l12;
   const bool use_a = (ax * ax + ay * ay) >= (bx * bx + by * by);
-  double vx = use_a ? ax : bx, vy = use_a ? ay : by;
+  vx = use_a ? ax : bx;
+  vy = use_a ? ay : by;
   const double n = sqrt(vx * vx + vy * vy);
   if (n == 0.0) { vx = 1.0; vy = 0.0; } else { vx /= n; vy /= n; }
+  const double det = f11 * f22 - f12 * f21;
+  lmin = lmax > 0.0 ? det * det / lmax : 0.0;
+}
+
+// Major eigenvector of L = F F^T per element.
+__global__ void k_fse_director(int64_t nel, const double* F, double* dxo, double* dyo) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= nel) return;
+  double vx, vy, l1, l2;
+  fse_axes(F[4 * e + 0], F[4 * e + 1], F[4 * e + 2], F[4 * e + 3], vx, vy, l1, l2);
   dxo[e] = vx;
   dyo[e] = vy;
 }

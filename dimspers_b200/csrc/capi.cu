@@ -34,6 +34,7 @@ Ctx::~Ctx() {
   cudaFree(flush);
   cudaFree(stress_buf);
   cudaFree(rheo_buf);
+  cudaFree(fabric_buf);
   cudaFree(scal); cudaFreeHost(h_scal); cudaFree(partial); cudaFree(counter);
   for (void* p : work) cudaFree(p);
   if (stream) cudaStreamDestroy(stream);
@@ -753,6 +754,7 @@ __global__ void k_flush_read(const uint4* __restrict__ buf, int64_t n, unsigned 
 namespace dp {
 void launch_stress_staged(Ctx& c, bool tensor);
 void launch_viscosity_staged(Ctx& c);
+void launch_dem_staged(Ctx& c);
 }
 
 int dp_profile_kernel(dp_ctx* h, int32_t which, int32_t reps, int32_t flush_l2, double* ms) {
@@ -766,7 +768,9 @@ int dp_profile_kernel(dp_ctx* h, int32_t which, int32_t reps, int32_t flush_l2, 
     if (which == 2 && c.mg.empty()) throw BadArg("no multigrid hierarchy (run a solve first)");
     if (which == 3 && !c.stress_buf) throw BadArg("no staged post-processor inputs (call dp_stress first)");
     if (which == 4 && !c.rheo_buf) throw BadArg("no staged viscosity inputs (call dp_viscosity_arrhenius first)");
-    if (which < 0 || which > 4) throw BadArg("which must be 0..4");
+    if (which == 5 && c.fabric_dem[0] == 0)
+      throw BadArg("no staged DEM tensor inputs (call dp_anisotropic_tensor first)");
+    if (which < 0 || which > 5) throw BadArg("which must be 0..5");
     const int64_t n = 2 * c.fine.nnod;
     double* x64 = (double*)c.work[W_IN_P];
     double* y64 = (double*)c.work[W_IN_AP];
@@ -783,6 +787,7 @@ int dp_profile_kernel(dp_ctx* h, int32_t which, int32_t reps, int32_t flush_l2, 
       else if (which == 1) launch_apply_K_acc<double, double>(c.fine, c.K64, x64, y64, c.stream);
       else if (which == 3) launch_stress_staged(c, c.stress_tensor);
       else if (which == 4) launch_viscosity_staged(c);
+      else if (which == 5) launch_dem_staged(c);
       else if (c.mg_prec == 1) mg_apply_f(c, x32, y32, MGOptions());
       else mg_apply(c, x64, y64, MGOptions());
     };

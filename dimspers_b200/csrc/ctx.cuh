@@ -116,6 +116,10 @@ struct Ctx {
   double* stress_buf = nullptr; // post-processor staging: eta 7, tensor 42, outputs 56 per element
   bool stress_tensor = false;   // the staged inputs carry a tensor
   double* rheo_buf = nullptr;   // viscosity update staging: 4 x 7 per element, 4 per node
+  double* fabric_buf = nullptr; // FSE / DEM tensor staging (fabric_cap doubles)
+  int64_t fabric_cap = 0;
+  int64_t fabric_dem[3] = {0, 0, 0};  // the last staged DEM table: nrows, n_a1a2, sblk (0: none)
+  double fabric_w = 0.0;
   double rheo_law[8] = {};      // the last viscosity update's law (eta0, R, Ea, Va, T0, sin, cos, phi)
 
   // multigrid hierarchy (level 0 = fine)

@@ -10,5 +10,6 @@
 #include "capi.cu"
 #include "stress.cu"
 #include "rheology.cu"
+#include "fabric.cu"
 #include "noalloc.cu"
 #include "cnn.cu"

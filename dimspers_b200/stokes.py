@@ -250,6 +250,35 @@ class StokesContext:
                                                _ptr(eta), DP_MEM_HOST))
         return np.array(eta)
 
+    def fse(self, F):
+        """getFSE (src/Stress/FSE.jl:131-161) per IP.  F: (nel, 6, 2, 2).
+        Returns dict vx1, vx2, vy1, vy2, a1, a2 of (nel, 6) arrays."""
+        F = np.asarray(F, dtype=np.float64)
+        if F.shape != (self.nel, 6, 2, 2):
+            raise ValueError("F must be (nel, 6, 2, 2)")
+        # Julia memory order: IP-major over elements, each 2x2 column-major
+        Fj = np.ascontiguousarray(F.transpose(1, 0, 3, 2))
+        outs = [np.empty((self.nel, 6), order="F") for _ in range(6)]
+        ptrs = (C.c_void_p * 6)(*[o.ctypes.data for o in outs])
+        self._chk(lib().dp_fse(self.h, _ptr(Fj), ptrs, self.nel, DP_MEM_HOST))
+        return dict(zip(("vx1", "vx2", "vy1", "vy2", "a1", "a2"), outs))
+
+    def anisotropic_tensor(self, dem, vx1, vy1, r1, r2):
+        """anisotropic_tensor (src/Rheology/anisotropy.jl:140-285) from the FSE
+        major axis and the fabric shape (r1, r2) per IP, (nel, 6) each, with
+        the DEM table `dem` (`dimspers_b200.fabric.DEM`).  Returns the six
+        StiffnessTensor fields, (nel, 7) each."""
+        ins = [np.asfortranarray(a, dtype=np.float64) for a in (vx1, vy1, r1, r2)]
+        for a in ins:
+            if a.shape != (self.nel, 6):
+                raise ValueError("inputs must be (nel, 6)")
+        outs = [np.empty((self.nel, 7), order="F") for _ in range(6)]
+        ptrs = (C.c_void_p * 6)(*[o.ctypes.data for o in outs])
+        d = dem.struct()
+        self._chk(lib().dp_anisotropic_tensor(self.h, C.byref(d), *[_ptr(a) for a in ins], self.nel, ptrs, self.nel,
+                                              DP_MEM_HOST))
+        return tuple(outs)
+
     def rhs(self):
         F = np.empty(2 * self.nnod)
         pc = np.empty(self.npres)
@@ -283,7 +312,8 @@ class StokesContext:
 
     def profile_kernel(self, which, reps=50, flush_l2=False):
         """Average ms per launch: 0 FP32 A-apply, 1 FP64 A-apply, 2 V-cycle,
-        3 stress post-processor, 4 viscosity update (last call's inputs);
+        3 stress post-processor, 4 viscosity update, 5 DEM tensor lookup (last
+        call's inputs);
         flush_l2 times each launch alone after overwriting 256 MB (cold L2)."""
         ms = C.c_double(0.0)
         self._chk(lib().dp_profile_kernel(self.h, int(which), int(reps), 1 if flush_l2 else 0, C.byref(ms)))

@@ -262,6 +262,40 @@ int dp_viscosity_arrhenius(dp_ctx* ctx, const dp_arrhenius* law, const double* T
                            int64_t nvert, const double* r_node, const double* epsII, const double* tauII,
                            const double* cohesion, double* eta_ip, int32_t mem);
 
+/* ---- per-IP finite-strain ellipsoid and DEM viscous tensor ---------------
+ * dp_fse: getFSE / _FSE (src/Stress/FSE.jl:131-161) at every IP: from the
+ * deformation gradient F (nel x 6 Julia SMatrix{2,2} per IP: F11, F21, F12,
+ * F22 at ((ip * nel) + e) * 4) to fse = {vx1, vx2, vy1, vy2, a1, a2}, each
+ * nel x ld_out element-fastest (columns 1..6 written): the major and minor
+ * eigenvectors of F F^T and the square roots of its eigenvalues.  The signs
+ * of the eigenvectors are not significant (the tensor depends on products of
+ * pairs of components only).
+ *
+ * dp_anisotropic_tensor: anisotropic_tensor (src/Rheology/anisotropy.jl:
+ * 140-285): per IP 1..6 the nearest row of the DEM table (argminsorted over
+ * a1a2_blk for the fabric shape r1 and over the sorted a2a3_blk for r2, row
+ * sblk (i1 - 1) + permutation_blk[i2]), its C11, C33, max(C55, w), C13 rotated
+ * by the FSE axis (vx1, vy1) with directRotation2D, eta55 floored at w; IP 7 =
+ * the mean of IPs 1..6.  vx1, vy1, r1, r2: nel x ld_in (columns 1..6 read);
+ * r1 = log10(a1/a2), r2 = log10(a2/a3) of the inclusion shape, as Fabrics.jl's
+ * fabric_shape(a1, 1, parameterization) returns it.  The table is in host
+ * memory: C is nrows x 9 column-major ([C11 C22 C33 C44 C55 C66 C12 C13 C23]),
+ * permutation_blk is 1-based, n_a1a2 * sblk <= nrows.  Out: the six
+ * StiffnessTensor fields (C11, C33, C55, C13, C15, C35), nel x ld_out. */
+typedef struct {
+  const double* C;
+  int64_t nrows;
+  const double* a1a2_blk;
+  int64_t n_a1a2;
+  const double* a2a3_blk;
+  const int64_t* permutation_blk;
+  int64_t sblk;
+  double w;
+} dp_dem;
+int dp_fse(dp_ctx* ctx, const double* F, double* const* fse, int64_t ld_out, int32_t mem);
+int dp_anisotropic_tensor(dp_ctx* ctx, const dp_dem* dem, const double* vx1, const double* vy1, const double* r1,
+                          const double* r2, int64_t ld_in, double* const* C6_out, int64_t ld_out, int32_t mem);
+
 /* ---- batches of independent solves ---------------------------------------
  * Independent problems (contexts of any resolution, all on one device) solved
  * by ONE graph launch: the batch graph holds one branch per context with that
@@ -307,7 +341,8 @@ int dp_guess_from_grid(dp_ctx* ctx, const float* p_grid, int32_t nrg, int32_t nt
  * FP32, 1 fine-level A-apply FP64, 2 one multigrid V-cycle (precision of the
  * last solve), 3 the stress post-processor on the inputs of the last
  * dp_stress call, 4 the viscosity update on the inputs of the last
- * dp_viscosity_arrhenius call.  flush_l2 = 0: `reps` back-to-back launches (warm L2);
+ * dp_viscosity_arrhenius call, 5 the DEM tensor lookup on the inputs of the
+ * last dp_anisotropic_tensor call.  flush_l2 = 0: `reps` back-to-back launches (warm L2);
  * 1: a 256 MB buffer is read before each launch and each launch is timed
  * alone (cold L2, DRAM-bound figure). */
 int dp_profile_kernel(dp_ctx* ctx, int32_t which, int32_t reps, int32_t flush_l2, double* ms_per_launch);

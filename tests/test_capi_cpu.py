@@ -99,13 +99,14 @@ def _header_struct_fields(name):
         decl = decl.strip()
         if not decl:
             continue
-        typ, names = decl.split(None, 1)
-        fields += [n.strip() for n in names.split(",")]
+        parts = decl.split(",")
+        fields += [parts[0].split()[-1].lstrip("*")] + [p.strip().lstrip("*") for p in parts[1:]]
     return fields
 
 
 @pytest.mark.parametrize("cname,pystruct", [("dp_solve_opts", "SolveOpts"), ("dp_solve_report", "SolveReport"),
-                                            ("dp_mesh_desc", "MeshDesc"), ("dp_arrhenius", "Arrhenius")])
+                                            ("dp_mesh_desc", "MeshDesc"), ("dp_arrhenius", "Arrhenius"),
+                                            ("dp_dem", "Dem")])
 def test_ctypes_structs_mirror_the_header(cname, pystruct):
     """The ctypes mirrors list the header's fields in the header's order."""
     py = [f for f, _ in getattr(_lib, pystruct)._fields_]

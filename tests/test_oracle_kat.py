@@ -202,3 +202,61 @@ def test_arrhenius_update_branches_scalar_restatement():
                 branches.add("creep")
             assert math.isclose(got[e, ip], want, rel_tol=1e-13), (e, ip)
     assert branches == {"yield", "kept", "creep"}
+
+
+def _dem_fixture(vol=30):
+    d = np.load(os.path.join(ROOT, "tests", "golden", "dem_1e-3_vol%d.npz" % vol))
+    return d["C"], d["ax"]
+
+
+def test_dem_tables_of_the_reference_files():
+    """getDEM's block structure on the reference's DEM tables (10 blocks of
+    10 rows), and the host-side DEM the C ABI receives agrees with the oracle."""
+    from oracle import fabric as OF
+    from dimspers_b200.fabric import DEM
+    for vol in (10, 20, 30):
+        C6, ax = _dem_fixture(vol)
+        t = OF.dem_tables(C6, ax)
+        assert t["sblk"] == 10 and len(t["a1a2_blk"]) == 10 and t["nblk"] == 11
+        assert np.all(np.diff(t["a1a2_blk"]) > 0) and np.all(np.diff(t["a2a3_blk"]) > 0)
+        assert sorted(t["permutation_blk"]) == list(range(1, 11))
+        d = DEM(C6, ax, w=1e-2)
+        assert d.sblk == t["sblk"]
+        np.testing.assert_array_equal(d.a1a2_blk, t["a1a2_blk"])
+        np.testing.assert_array_equal(d.a2a3_blk, t["a2a3_blk"])
+        np.testing.assert_array_equal(d.permutation_blk, t["permutation_blk"])
+
+
+def test_dem_tensor_at_table_points_is_the_table_row():
+    """Shapes exactly at table points and an unrotated FSE (vx1 = 1, vy1 = 0)
+    return the table row itself: (C11, C33, max(C55, w), C13, 0, 0)."""
+    from oracle import fabric as OF
+    C6, ax = _dem_fixture()
+    t = OF.dem_tables(C6, ax)
+    w = 0.02
+    rows = [0, 13, 57, 99, 42]
+    r1 = np.array([[np.log10(ax[k, 0])] * 6 for k in rows])
+    r2 = np.array([[np.log10(1.0 / ax[k, 2])] * 6 for k in rows])
+    one, zero = np.ones_like(r1), np.zeros_like(r1)
+    out = OF.anisotropic_tensor(one, zero, r1, r2, t, w)
+    for j, k in enumerate(rows):
+        want = (C6[k, 0], C6[k, 2], max(C6[k, 4], w), C6[k, 7], 0.0, 0.0)
+        for f in range(6):
+            assert np.allclose(out[f][j], want[f], rtol=0, atol=1e-15), (k, f)
+    # argminsorted's first-local-minimum rule, including ties and the last index
+    assert OF.argminsorted(np.array([3.0, 2.0, 2.0, 5.0])) == 2
+    assert OF.argminsorted(np.array([3.0, 2.0, 1.0])) == 2
+    assert OF.argminsorted(np.array([1.0, 2.0, 0.0])) == 0
+
+
+def test_fse_of_a_rotated_stretch():
+    from oracle import fabric as OF
+    rng = np.random.default_rng(5)
+    ang = rng.uniform(-np.pi, np.pi, (4, 6))
+    s1, s2 = rng.uniform(1, 5, (4, 6)), rng.uniform(0.1, 1, (4, 6))
+    c, s = np.cos(ang), np.sin(ang)
+    R = np.stack([np.stack([c, -s], -1), np.stack([s, c], -1)], -2)
+    F = R @ (np.eye(2) * np.stack([s1, s2], -1)[..., None, :])    # R diag(s1, s2): major axis (c, s)
+    x1, x2, y1, y2, a1, a2 = OF.fse(F)
+    assert np.allclose(a1, s1) and np.allclose(a2, s2)
+    assert np.allclose(np.abs(x1 * c + y1 * s), 1.0) and np.allclose(x1 * x2 + y1 * y2, 0.0, atol=1e-12)
