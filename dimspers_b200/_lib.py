@@ -42,6 +42,12 @@ class Arrhenius(C.Structure):
                 ("T0", C.c_double), ("phi_deg", C.c_double)]
 
 
+class ThermalOpts(C.Structure):
+    _fields_ = [("K", C.c_double), ("Cp", C.c_double), ("dt", C.c_double), ("Ttop", C.c_double),
+                ("Tbot", C.c_double), ("rtol", C.c_double), ("atol", C.c_double), ("heated", C.c_int32),
+                ("itmax", C.c_int32)]
+
+
 class Dem(C.Structure):
     _fields_ = [("C", C.c_void_p), ("nrows", C.c_int64), ("a1a2_blk", C.c_void_p), ("n_a1a2", C.c_int64),
                 ("a2a3_blk", C.c_void_p), ("permutation_blk", C.c_void_p), ("sblk", C.c_int64), ("w", C.c_double)]
@@ -90,6 +96,9 @@ SIGNATURES = {
     "dp_profile_kernel": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     "dp_stress": (C.c_int, [_P, _P, _P, C.c_int64, C.POINTER(_P), C.c_int64, _P, C.c_int32]),
     "dp_viscosity_arrhenius": (C.c_int, [_P, C.POINTER(Arrhenius), _P, _P, C.c_int64, _P, _P, _P, _P, _P, C.c_int32]),
+    "dp_default_thermal_opts": (None, [C.POINTER(ThermalOpts)]),
+    "dp_thermal_step": (C.c_int, [_P, C.POINTER(ThermalOpts), _P, _P, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                  C.c_int32]),
     "dp_fse": (C.c_int, [_P, _P, C.POINTER(_P), C.c_int64, C.c_int32]),
     "dp_anisotropic_tensor": (C.c_int, [_P, C.POINTER(Dem), _P, _P, _P, _P, C.c_int64, C.POINTER(_P), C.c_int64,
                                         C.c_int32]),

@@ -35,6 +35,8 @@ Ctx::~Ctx() {
   cudaFree(stress_buf);
   cudaFree(rheo_buf);
   cudaFree(fabric_buf);
+  if (th_exec) cudaGraphExecDestroy((cudaGraphExec_t)th_exec);
+  cudaFree(th_buf);
   cudaFree(scal); cudaFreeHost(h_scal); cudaFree(partial); cudaFree(counter);
   for (void* p : work) cudaFree(p);
   if (stream) cudaStreamDestroy(stream);
@@ -755,6 +757,7 @@ namespace dp {
 void launch_stress_staged(Ctx& c, bool tensor);
 void launch_viscosity_staged(Ctx& c);
 void launch_dem_staged(Ctx& c);
+void launch_th_apply_staged(Ctx& c);
 }
 
 int dp_profile_kernel(dp_ctx* h, int32_t which, int32_t reps, int32_t flush_l2, double* ms) {
@@ -770,7 +773,8 @@ int dp_profile_kernel(dp_ctx* h, int32_t which, int32_t reps, int32_t flush_l2, 
     if (which == 4 && !c.rheo_buf) throw BadArg("no staged viscosity inputs (call dp_viscosity_arrhenius first)");
     if (which == 5 && c.fabric_dem[0] == 0)
       throw BadArg("no staged DEM tensor inputs (call dp_anisotropic_tensor first)");
-    if (which < 0 || which > 5) throw BadArg("which must be 0..5");
+    if (which == 6 && !c.th_buf) throw BadArg("no thermal element blocks (call dp_thermal_step first)");
+    if (which < 0 || which > 6) throw BadArg("which must be 0..6");
     const int64_t n = 2 * c.fine.nnod;
     double* x64 = (double*)c.work[W_IN_P];
     double* y64 = (double*)c.work[W_IN_AP];
@@ -788,6 +792,7 @@ int dp_profile_kernel(dp_ctx* h, int32_t which, int32_t reps, int32_t flush_l2, 
       else if (which == 3) launch_stress_staged(c, c.stress_tensor);
       else if (which == 4) launch_viscosity_staged(c);
       else if (which == 5) launch_dem_staged(c);
+      else if (which == 6) launch_th_apply_staged(c);
       else if (c.mg_prec == 1) mg_apply_f(c, x32, y32, MGOptions());
       else mg_apply(c, x64, y64, MGOptions());
     };

@@ -120,6 +120,9 @@ struct Ctx {
   int64_t fabric_cap = 0;
   int64_t fabric_dem[3] = {0, 0, 0};  // the last staged DEM table: nrows, n_a1a2, sblk (0: none)
   double fabric_w = 0.0;
+  double* th_buf = nullptr;     // thermal step: 21 x nel element blocks + 10 nnod vectors
+  void* th_exec = nullptr;      // cudaGraphExec_t of the thermal CG loop
+  int th_heated = -1;           // wall configuration the loop graph was captured for
   double rheo_law[8] = {};      // the last viscosity update's law (eta0, R, Ea, Va, T0, sin, cos, phi)
 
   // multigrid hierarchy (level 0 = fine)

@@ -11,5 +11,6 @@
 #include "stress.cu"
 #include "rheology.cu"
 #include "fabric.cu"
+#include "thermal.cu"
 #include "noalloc.cu"
 #include "cnn.cu"

@@ -250,6 +250,28 @@ class StokesContext:
                                                _ptr(eta), DP_MEM_HOST))
         return np.array(eta)
 
+    def thermal_step(self, T, rho_node, dt, **opts):
+        """solveDiffusion_threaded (AssemblerThermal.jl:1-57): one backward-Euler
+        step of the nodal temperature T (reference numbering).  opts: K, Cp,
+        Ttop, Tbot, heated, rtol, atol, itmax (defaults: dp_default_thermal_opts).
+        Returns (T_new, iterations, relres)."""
+        o = _lib.ThermalOpts()
+        lib().dp_default_thermal_opts(C.byref(o))
+        o.dt = float(dt)
+        for k, v in opts.items():
+            if not hasattr(o, k):
+                raise KeyError(k)
+            setattr(o, k, v)
+        Tn = np.array(T, dtype=np.float64, copy=True)
+        rho = np.ascontiguousarray(rho_node, dtype=np.float64)
+        if Tn.shape != (self.nnod,) or rho.shape != (self.nnod,):
+            raise ValueError("T and rho_node must hold nnod values")
+        it = C.c_int32(0)
+        rel = C.c_double(0.0)
+        self._chk(lib().dp_thermal_step(self.h, C.byref(o), _ptr(rho), _ptr(Tn), C.byref(it), C.byref(rel),
+                                        DP_MEM_HOST))
+        return Tn, it.value, rel.value
+
     def fse(self, F):
         """getFSE (src/Stress/FSE.jl:131-161) per IP.  F: (nel, 6, 2, 2).
         Returns dict vx1, vx2, vy1, vy2, a1, a2 of (nel, 6) arrays."""
@@ -312,8 +334,8 @@ class StokesContext:
 
     def profile_kernel(self, which, reps=50, flush_l2=False):
         """Average ms per launch: 0 FP32 A-apply, 1 FP64 A-apply, 2 V-cycle,
-        3 stress post-processor, 4 viscosity update, 5 DEM tensor lookup (last
-        call's inputs);
+        3 stress post-processor, 4 viscosity update, 5 DEM tensor lookup, 6
+        thermal apply (last call's inputs);
         flush_l2 times each launch alone after overwriting 256 MB (cold L2)."""
         ms = C.c_double(0.0)
         self._chk(lib().dp_profile_kernel(self.h, int(which), int(reps), 1 if flush_l2 else 0, C.byref(ms)))

@@ -292,6 +292,24 @@ typedef struct {
   int64_t sblk;
   double w;
 } dp_dem;
+/* ---- thermal diffusion step ---------------------------------------------
+ * solveDiffusion_threaded (src/ThermalDiffusion/AssemblerThermal.jl:1-57):
+ * backward Euler (M + dt K) T_new = M T_old with M the rho Cp mass and K the
+ * conduction matrix of the P2 elements (7-point rule), T fixed to Ttop on the
+ * outer wall and, if heated, Tbot on the inner one (heated_bottom /
+ * insulated_bottom, boundary_conditions.jl:77-105).  Stopping test ||r|| <=
+ * atol + rtol ||b|| (Krylov.jl's defaults: sqrt(eps) both).  rho_node: nodal
+ * density (vertices read); T: nnod, reference numbering, T_old in, T_new out.
+ * Returns DP_NOT_CONVERGED when itmax iterations did not meet the test.
+ * itmax = 0: the number of nodes. */
+typedef struct {
+  double K, Cp, dt, Ttop, Tbot, rtol, atol;
+  int32_t heated, itmax;
+} dp_thermal_opts;
+void dp_default_thermal_opts(dp_thermal_opts* opts);
+int dp_thermal_step(dp_ctx* ctx, const dp_thermal_opts* opts, const double* rho_node, double* T,
+                    int32_t* iterations, double* relres, int32_t mem);
+
 int dp_fse(dp_ctx* ctx, const double* F, double* const* fse, int64_t ld_out, int32_t mem);
 int dp_anisotropic_tensor(dp_ctx* ctx, const dp_dem* dem, const double* vx1, const double* vy1, const double* r1,
                           const double* r2, int64_t ld_in, double* const* C6_out, int64_t ld_out, int32_t mem);
@@ -342,7 +360,8 @@ int dp_guess_from_grid(dp_ctx* ctx, const float* p_grid, int32_t nrg, int32_t nt
  * last solve), 3 the stress post-processor on the inputs of the last
  * dp_stress call, 4 the viscosity update on the inputs of the last
  * dp_viscosity_arrhenius call, 5 the DEM tensor lookup on the inputs of the
- * last dp_anisotropic_tensor call.  flush_l2 = 0: `reps` back-to-back launches (warm L2);
+ * last dp_anisotropic_tensor call, 6 the thermal element-by-element apply
+ * (A p of the last dp_thermal_step's blocks).  flush_l2 = 0: `reps` back-to-back launches (warm L2);
  * 1: a 256 MB buffer is read before each launch and each launch is timed
  * alone (cold L2, DRAM-bound figure). */
 int dp_profile_kernel(dp_ctx* ctx, int32_t which, int32_t reps, int32_t flush_l2, double* ms_per_launch);

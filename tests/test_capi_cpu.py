@@ -106,7 +106,8 @@ def _header_struct_fields(name):
 
 @pytest.mark.parametrize("cname,pystruct", [("dp_solve_opts", "SolveOpts"), ("dp_solve_report", "SolveReport"),
                                             ("dp_mesh_desc", "MeshDesc"), ("dp_arrhenius", "Arrhenius"),
-                                            ("dp_dem", "Dem")])
+                                            ("dp_dem", "Dem"),
+                                            ("dp_thermal_opts", "ThermalOpts")])
 def test_ctypes_structs_mirror_the_header(cname, pystruct):
     """The ctypes mirrors list the header's fields in the header's order."""
     py = [f for f, _ in getattr(_lib, pystruct)._fields_]

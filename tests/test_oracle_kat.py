@@ -260,3 +260,34 @@ def test_fse_of_a_rotated_stretch():
     x1, x2, y1, y2, a1, a2 = OF.fse(F)
     assert np.allclose(a1, s1) and np.allclose(a2, s2)
     assert np.allclose(np.abs(x1 * c + y1 * s), 1.0) and np.allclose(x1 * x2 + y1 * y2, 0.0, atol=1e-12)
+
+
+def test_thermal_element_blocks():
+    """assemble_element! (AssemblerThermal.jl:114-226) restated: constants are
+    the conduction block's null space, the mass blocks integrate rho Cp over
+    the annulus, both symmetric (K positive semi-definite)."""
+    from oracle import thermal as OT
+    prob = OS.make_problem(4, 32, "continuous")
+    gr = prob.gr
+    Ke, Me = OT.element_matrices(prob.th, prob.r, np.full(gr.nnod, 2.0), gr.e2n, 1.7, 3.0)
+    assert np.abs(Ke.sum(axis=2)).max() < 1e-12
+    assert math.isclose(Me.sum(), 6.0 * math.pi * (2.22 ** 2 - 1.22 ** 2), rel_tol=1e-12)
+    assert np.abs(Ke - Ke.transpose(0, 2, 1)).max() < 1e-12 and np.abs(Me - Me.transpose(0, 2, 1)).max() < 1e-14
+    assert np.linalg.eigvalsh(Ke).min() > -1e-12
+
+
+def test_thermal_long_step_converges_to_conduction_profile():
+    """A very long backward-Euler step is the steady conduction solution
+    T = Tbot + (Ttop - Tbot) ln(r / r_in) / ln(r_out / r_in); the P2 error
+    falls by ~8x per refinement."""
+    from oracle import thermal as OT
+    errs = []
+    for nr, nt in ((4, 32), (8, 64)):
+        prob = OS.make_problem(nr, nt, "continuous")
+        gr = prob.gr
+        fixed, tfix = OT.boundary(gr, 300.0, 4000.0)
+        T = OT.thermal_step(gr, prob.th, prob.r, np.full(gr.nnod, 1000.0), np.ones(gr.nnod), 1.0, 1.0, 1e9,
+                            fixed, tfix)
+        exact = 4000.0 + (300.0 - 4000.0) * np.log(gr.r / 1.22) / np.log(2.22 / 1.22)
+        errs.append(np.abs(T - exact).max())
+    assert errs[1] < errs[0] / 6 and errs[1] < 0.05
