@@ -74,3 +74,26 @@ def test_arrhenius_viscosity_update_matches_oracle():
     assert np.abs(got / ref - 1).max() < 1e-12
     kept = ref == 3.3e21
     assert kept.any() and (ref == 1e18).any() and (~kept & (ref > 1e18)).any()
+
+
+def test_stress_properties_at_128x1024():
+    """Size-independent properties at the benchmark mesh: a rigid rotation
+    (u = omega x r) has no strain rate and a Cartesian-linear field has its
+    constant strain rate and stress, up to the second-order error of the P2
+    space on elements straight in (theta, r) (6.1e-4 and 1.3e-3 at 8x64, 4x
+    less per refinement: ~2.4e-6 and 5e-6 here)."""
+    from dimspers_b200 import StokesContext, build_mesh
+    mesh = build_mesh(128, 1024, "discontinuous", colors=False)
+    x, z = mesh.r * np.sin(mesh.theta), mesh.r * np.cos(mesh.theta)
+    eta = np.full((mesh.nel, 7), 2.0)
+    with StokesContext(128, 1024, "discontinuous") as ctx:
+        U = np.zeros(2 * mesh.nnod)
+        U[0::2], U[1::2] = 0.7 * z, -0.7 * x                   # rigid rotation
+        rot = ctx.stress(U, eta)
+        U[0::2], U[1::2] = 0.3 * x + 0.2 * z, 0.5 * x - 0.3 * z  # exx = 0.3, ezz = -0.3, exz = 0.35
+        lin = ctx.stress(U, eta)
+    assert max(np.abs(rot[k]).max() for k in ("exx", "ezz", "exz", "eII")) < 1e-5
+    for k, v in (("exx", 0.3), ("ezz", -0.3), ("exz", 0.35)):
+        assert np.abs(lin[k] - v).max() < 1e-5, k
+    assert np.abs(lin["txx"] - 2.0 * (4 / 3 * 0.3 + 2 / 3 * 0.3)).max() < 2e-5
+    assert np.abs(lin["txz"] - 2.0 * 2 * 0.35).max() < 2e-5

@@ -54,3 +54,18 @@ def test_thermal_step_repeats_and_reports():
     fixed, tfix = OT.boundary(prob.gr, 300.0, 4000.0)
     inside = np.setdiff1d(np.arange(prob.gr.nnod), fixed)
     assert np.abs(T0[inside] - T[inside]).max() / np.abs(T).max() < 1e-2
+
+
+def test_thermal_long_step_at_128x1024():
+    """At the benchmark mesh a very long step is the steady conduction profile
+    (the P2 error falls as h^4: 1.7e-5 K at 32x256, ~1e-7 K here; the bound
+    leaves room for the solver's kappa * rtol), and the walls hold their values."""
+    from dimspers_b200 import StokesContext
+    with StokesContext(128, 1024, "continuous") as ctx:
+        r = ctx.mesh.r
+        T0 = np.full(ctx.nnod, 1000.0)
+        T, it, rel = ctx.thermal_step(T0, np.ones(ctx.nnod), 1e9, K=1.0, Cp=1.0, rtol=1e-13, atol=0.0,
+                                      itmax=200000)
+    exact = 4000.0 + (300.0 - 4000.0) * np.log(r / 1.22) / np.log(2.22 / 1.22)
+    assert np.abs(T - exact).max() < 5e-3
+    assert np.all(T[r == r.max()] == 300.0) and np.all(T[r == r.min()] == 4000.0)
