@@ -5,7 +5,8 @@
 //
 // k_fse_ip: one thread per (IP, element), the closed-form eigen-decomposition
 // of L = F F^T shared with the per-element director.
-// k_dem_tensor: one thread per element (IP 7 is the mean of IPs 1..6).  Per
+// k_dem_tensor: one warp per (IP, 32 elements), IP 7 the mean of IPs 1..6
+// through shared memory.  Per
 // IP the nearest DEM row by the reference's argminsorted scans (first i with
 // |r - b[i]| < |r - b[i+1]|, the same comparisons on the same values, so the
 // row chosen is the reference's), then directRotation2D by the FSE axis.  The
@@ -70,14 +71,18 @@ __device__ __forceinline__ void direct_rotation_2d(double cosa, double sina, dou
   n[5] = ((c * y2y2 + h * y1y1) * x2 + 2 * m * e * y1) * y2 + (a * y1y1 + h * y2y2) * x1 * y1;
 }
 
-// in: field-major 4 x 6 nel (vx1, vy1, r1, r2; ip * nel + e); out: 6 x 7 nel
-__global__ void __launch_bounds__(128) k_dem_tensor(const double* __restrict__ in, double* __restrict__ out, DemDev d,
-                                                     int nel) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= nel) return;
+constexpr int kDemEl = 32;  // elements per CTA: warps 0..5 one IP each, warp 6 the IP-7 mean
+
+// in: field-major 4 x 6 nel (vx1, vy1, r1, r2; ip * nel + e); out: 6 x 7 nel.
+// Every load and store is a coalesced row of an element-fastest matrix.
+__global__ void __launch_bounds__(kDemEl * 7) k_dem_tensor(const double* __restrict__ in, double* __restrict__ out,
+                                                           DemDev d, int nel) {
+  __shared__ double sh[6][6][kDemEl];  // field, ip, element
+  const int tx = threadIdx.x, ip = threadIdx.y;
+  const int e = blockIdx.x * kDemEl + tx;
+  const bool valid = e < nel;
   const size_t st = (size_t)nel, n6 = 6 * st, n7 = 7 * st;
-  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int ip = 0; ip < 6; ++ip) {
+  if (valid && ip < 6) {
     const size_t i = (size_t)ip * st + e;
     const double x = in[i], y = in[n6 + i], r1 = in[2 * n6 + i], r2 = in[3 * n6 + i];
     const int i1 = argmin_sorted(r1, d.b1, d.n1);
@@ -92,11 +97,19 @@ __global__ void __launch_bounds__(128) k_dem_tensor(const double* __restrict__ i
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
       out[k * n7 + i] = n[k];
-      acc[k] += n[k];
+      sh[k][ip][tx] = n[k];
     }
   }
+  __syncthreads();
+  if (valid && ip == 6) {
 #pragma unroll
-  for (int k = 0; k < 6; ++k) out[k * n7 + 6 * st + e] = acc[k] * (1.0 / 6.0);
+    for (int k = 0; k < 6; ++k) {
+      double acc = 0.0;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) acc += sh[k][q][tx];
+      out[k * n7 + 6 * st + e] = acc * (1.0 / 6.0);
+    }
+  }
 }
 
 static DemDev staged_dem(Ctx& c, double* tab) {
@@ -115,7 +128,7 @@ static DemDev staged_dem(Ctx& c, double* tab) {
 static void launch_k_dem_tensor(Ctx& c, const double* in, double* o, const DemDev& d) {
   const int64_t nel = c.fine.nel;
   ++g_klaunch;
-  k_dem_tensor<<<(int)div_up(nel, 128), 128, 0, c.stream>>>(in, o, d, (int)nel);
+  k_dem_tensor<<<(int)div_up(nel, kDemEl), dim3(kDemEl, 7), 0, c.stream>>>(in, o, d, (int)nel);
   DP_LAUNCH_CHECK();
 }
 

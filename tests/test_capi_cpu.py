@@ -125,3 +125,17 @@ def test_default_opts_fill_exactly_the_struct():
     o = _lib.SolveOpts.from_buffer(buf)
     assert (o.rtol, o.itmax, o.itmin, o.cheb_degree, o.coarse_max) == (1e-8, 200, 10, 3, 1536)
     assert (o.launch_overlap, o.true_residual, o.matrix_free, o.mg_tail, o.relax_base) == (1, 1, 0, 0, 0.0)
+
+
+def test_default_thermal_opts():
+    """dp_default_thermal_opts fills exactly the struct: MAIN.jl's thermal
+    parameters (K = 3.3, Cp = 1.2e3, walls 300 / 4000, heated) and Krylov.jl's
+    default tolerances sqrt(eps)."""
+    import ctypes as C
+    n = C.sizeof(_lib.ThermalOpts)
+    buf = (C.c_ubyte * (n + 32))(*([0xCD] * (n + 32)))
+    _lib.lib().dp_default_thermal_opts(C.cast(buf, C.POINTER(_lib.ThermalOpts)))
+    assert bytes(buf[n:]) == bytes([0xCD] * 32)
+    o = _lib.ThermalOpts.from_buffer(buf)
+    assert (o.K, o.Cp, o.Ttop, o.Tbot, o.heated, o.itmax) == (3.3, 1.2e3, 300.0, 4000.0, 1, 0)
+    assert o.rtol == o.atol == np.sqrt(np.finfo(np.float64).eps)
