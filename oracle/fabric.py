@@ -88,7 +88,7 @@ def fse(F):
     eigenvector signs are those of LAPACK here and are not significant."""
     L = np.einsum("...ik,...jk->...ij", F, F)
     lam, vec = np.linalg.eigh(L)                 # ascending
-    imax = np.where(lam[..., 1] >= lam[..., 0], 1, 0)
+    imax = np.where(lam[..., 1] > lam[..., 0], 1, 0)      # eigval_order: ties keep the first
     imin = 1 - imax
     take = lambda a, i: np.take_along_axis(a, i[..., None], axis=-1)[..., 0]  # noqa: E731
     x1 = take(vec[..., 0, :], imax)
