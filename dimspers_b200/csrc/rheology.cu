@@ -2,7 +2,7 @@
 // getviscosity!(::Arrhenius, T, P, epsII, tauII, e2n, r) (src/Rheology/
 // Rheology.jl:348-403), the producer of the eta.ip the Stokes assembly reads.
 //
-// One warp per (IP, 32 elements), 7-point IPs (Quadrature.jl:109-138): T_ip and the
+// One thread per element, 7-point IPs (Quadrature.jl:109-138): T_ip and the
 // radius z_ip by the P2 shape functions, P_ip by the linear ones at the three
 // vertices plus |min P| (a device reduction), a depth factor lambda (1e1
 // between max r - 2780 km and max r - 660 km, 1e-3 below, 1e0 above), eta_TP =
@@ -79,48 +79,49 @@ struct ArrheniusArgs {
   double eta0, R, Ea, Va, T0, sphi, cphi, phi;
 };
 
-constexpr int kViscEl = 32;  // elements per CTA, one warp per IP
-
 // T, P (vertex entries; others unused), r: lattice order.  epsII, tauII, coh,
-// eta: nel x 7 element-fastest.  One warp per (IP, 32 elements): coalesced
-// rows of the IP matrices, the element's node gathers shared through L1.
-__global__ void __launch_bounds__(kViscEl * 7) k_viscosity_arrhenius(
-    const double* __restrict__ T, const double* __restrict__ P, const double* __restrict__ r,
-    const double* __restrict__ epsII, const double* __restrict__ tauII, const double* __restrict__ coh,
-    double* __restrict__ eta, const double* __restrict__ scal, ArrheniusArgs law, int nel, int ncr, int A, int B) {
-  const int e = blockIdx.x * kViscEl + threadIdx.x;
-  const int ip = threadIdx.y;
+// eta: nel x 7 element-fastest.
+__global__ void __launch_bounds__(128) k_viscosity_arrhenius(const double* __restrict__ T, const double* __restrict__ P,
+                                                             const double* __restrict__ r,
+                                                             const double* __restrict__ epsII,
+                                                             const double* __restrict__ tauII,
+                                                             const double* __restrict__ coh, double* __restrict__ eta,
+                                                             const double* __restrict__ scal, ArrheniusArgs law,
+                                                             int nel, int ncr, int A, int B) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nel) return;
-  const size_t i = (size_t)ip * nel + e;
-  const double e2 = epsII[i], c = coh[i], tau = tauII[i], eta_prev = eta[i];
   int64_t nd[6];
   element_nodes(e, ncr, A, B, nd);
-  double T_ip = 0.0, z_ip = 0.0;
+  double Te[6], re[6], Pe[3];
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
-    T_ip += T[nd[k]] * c_N6s[ip][k];
-    z_ip += r[nd[k]] * c_N6s[ip][k];
+    Te[k] = T[nd[k]];
+    re[k] = r[nd[k]];
   }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) Pe[k] = P[nd[k]];
   const double minP = scal[S_MINP], maxr = scal[S_MAXR];
-  const double P_ip = P[nd[0]] * c_N3s[ip][0] + P[nd[1]] * c_N3s[ip][1] + P[nd[2]] * c_N3s[ip][2] + minP;
-  const double lam = z_ip < maxr - 2780e3 ? 1e-3 : (z_ip > maxr - 660e3 ? 1e0 : 1e1);
-  const double etaTP =
-      fmin(fmax(lam * law.eta0 * exp((law.Ea + P_ip * law.Va) / law.R / T_ip - law.Ea / law.R / law.T0), 1e18), 1e25);
-  double out = etaTP;
-  if (c > 0.0 && law.phi > 0.0 && e2 != 0.0) {
-    const double tau_y = law.cphi * c + law.sphi * P_ip;
-    out = tau_y < tau ? fmax(1e18, fmin(1e25, 0.5 * tau_y / e2)) : eta_prev;
+  const size_t st = (size_t)nel;
+  for (int ip = 0; ip < 7; ++ip) {
+    double T_ip = 0.0, z_ip = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      T_ip += Te[k] * c_N6s[ip][k];
+      z_ip += re[k] * c_N6s[ip][k];
+    }
+    const double P_ip = Pe[0] * c_N3s[ip][0] + Pe[1] * c_N3s[ip][1] + Pe[2] * c_N3s[ip][2] + minP;
+    const double lam = z_ip < maxr - 2780e3 ? 1e-3 : (z_ip > maxr - 660e3 ? 1e0 : 1e1);
+    const double etaTP =
+        fmin(fmax(lam * law.eta0 * exp((law.Ea + P_ip * law.Va) / law.R / T_ip - law.Ea / law.R / law.T0), 1e18), 1e25);
+    const size_t i = (size_t)ip * st + e;
+    const double e2 = epsII[i], c = coh[i];
+    if (c > 0.0 && law.phi > 0.0 && e2 != 0.0) {
+      const double tau_y = law.cphi * c + law.sphi * P_ip;
+      if (tau_y < tauII[i]) eta[i] = fmax(1e18, fmin(1e25, 0.5 * tau_y / e2));
+    } else {
+      eta[i] = etaTP;
+    }
   }
-  eta[i] = out;
-}
-
-static void launch_k_viscosity(Ctx& c, const double* T, const double* P, const double* r, const double* e2,
-                               const double* t2, const double* co, double* et, const ArrheniusArgs& a) {
-  const int64_t nel = c.fine.nel;
-  ++g_klaunch;
-  k_viscosity_arrhenius<<<(int)div_up(nel, kViscEl), dim3(kViscEl, 7), 0, c.stream>>>(
-      T, P, r, e2, t2, co, et, c.scal, a, (int)nel, c.fine.ncr, (int)c.fine.A(), (int)c.fine.B());
-  DP_LAUNCH_CHECK();
 }
 
 // k_viscosity_arrhenius on the inputs staged by the last dp_viscosity_arrhenius
@@ -133,7 +134,12 @@ void launch_viscosity_staged(Ctx& c) {
   ArrheniusArgs a;
   a.eta0 = c.rheo_law[0]; a.R = c.rheo_law[1]; a.Ea = c.rheo_law[2]; a.Va = c.rheo_law[3];
   a.T0 = c.rheo_law[4]; a.sphi = c.rheo_law[5]; a.cphi = c.rheo_law[6]; a.phi = c.rheo_law[7];
-  launch_k_viscosity(c, Tl, Tl + nn, Tl + 2 * nn, e2, e2 + 7 * nel, e2 + 14 * nel, e2 + 21 * nel, a);
+  ++g_klaunch;
+  k_viscosity_arrhenius<<<(int)div_up(nel, 128), 128, 0, c.stream>>>(Tl, Tl + nn, Tl + 2 * nn, e2, e2 + 7 * nel,
+                                                                      e2 + 14 * nel, e2 + 21 * nel, c.scal, a,
+                                                                      (int)nel, c.fine.ncr, (int)c.fine.A(),
+                                                                      (int)c.fine.B());
+  DP_LAUNCH_CHECK();
 }
 
 }  // namespace dp
@@ -192,7 +198,10 @@ extern "C" int dp_viscosity_arrhenius(dp_ctx* h, const dp_arrhenius* law, const 
     a.cphi = std::cos(law->phi_deg * (3.14159265358979323846 / 180.0));
     const double keep[8] = {a.eta0, a.R, a.Ea, a.Va, a.T0, a.sphi, a.cphi, a.phi};
     for (int i = 0; i < 8; ++i) c.rheo_law[i] = keep[i];
-    launch_k_viscosity(c, Tl, Pl, rl, e2, t2, co, et, a);
+    ++g_klaunch;
+    k_viscosity_arrhenius<<<(int)div_up(nel, 128), 128, 0, c.stream>>>(Tl, Pl, rl, e2, t2, co, et, c.scal, a, (int)nel,
+                                                                        c.fine.ncr, (int)c.fine.A(), (int)c.fine.B());
+    DP_LAUNCH_CHECK();
     DP_CUDA(cudaMemcpyAsync(eta_ip, et, sizeof(double) * 7 * nel, kind_out(mem), c.stream));
     DP_CUDA(cudaStreamSynchronize(c.stream));
     return (int)DP_OK;

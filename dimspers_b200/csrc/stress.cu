@@ -2,10 +2,7 @@
 // 23-249), called after each Stokes solve with the Cartesian velocity
 // (MAIN.jl:241-243, nip = 7: MAIN.jl:94, :164).
 //
-// One warp per (IP, 32 elements), the 7 IPs of 32 elements in one CTA of
-// 7 warps (FP64): every load and store is a coalesced 256-byte row of an
-// element-fastest matrix, and the element's velocity and vertex gathers are
-// shared by the 7 warps through L1.  Per 7-point IP: the curved inverse Jacobian
+// One thread per element (FP64).  Per 7-point IP: the curved inverse Jacobian
 // of the (theta, r)-linear element (the same geometry as the assembly), the P2
 // derivatives dN/dx, dN/dz, the strain rate (exx, ezz, exz = (dux/dz +
 // duz/dx) / 2) and its second invariant, and the deviatoric stress with its
@@ -39,18 +36,13 @@ static void upload_stress_constants() {
   DP_CUDA(cudaMemcpyToSymbol(c_dNs, dN, sizeof(dN)));
 }
 
-constexpr int kStressEl = 32;  // elements per CTA (one warp per IP)
-
 // U: Cartesian velocity, lattice order, interleaved (ux, uz).  eta: 7*nel
 // (ip-major), C: 42*nel ((field*7 + ip)*nel + e) or null.  out: 56*nel.
-__global__ void __launch_bounds__(kStressEl * 7) k_stress(const double* __restrict__ U,
-                                                          const double* __restrict__ theta_lat,
-                                                          const double* __restrict__ r_lat,
-                                                          const double* __restrict__ eta,
-                                                          const double* __restrict__ C, double* __restrict__ out,
-                                                          int nel, int ncr, int A, int B) {
-  const int e = blockIdx.x * kStressEl + threadIdx.x;
-  const int ip = threadIdx.y;
+__global__ void __launch_bounds__(128) k_stress(const double* __restrict__ U, const double* __restrict__ theta_lat,
+                                                const double* __restrict__ r_lat, const double* __restrict__ eta,
+                                                const double* __restrict__ C, double* __restrict__ out, int nel,
+                                                int ncr, int A, int B) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nel) return;
   const int q = e >> 1, t = e & 1;
   const int ir = q % ncr, it = q / ncr;
@@ -62,15 +54,6 @@ __global__ void __launch_bounds__(kStressEl * 7) k_stress(const double* __restri
   } else {
     aa[0] = a0; aa[1] = a0 + 2; aa[2] = a0 + 2; aa[3] = a0 + 1; aa[4] = a0 + 2; aa[5] = a0 + 1;
     bb[0] = b0 + 2; bb[1] = b0 + 2; bb[2] = b0; bb[3] = b0 + 2; bb[4] = b0 + 1; bb[5] = b0 + 1;
-  }
-  const size_t st = (size_t)nel;
-  const size_t i = (size_t)ip * st + e;
-  // the IP's own inputs first: independent of the gathers below
-  const double et = eta[i];
-  double cf[6];
-  if (C) {
-#pragma unroll
-    for (int f = 0; f < 6; ++f) cf[f] = C[(size_t)(f * 7) * st + i] * et;
   }
   int nd[6];
   double ux[6], uz[6];
@@ -103,54 +86,52 @@ __global__ void __launch_bounds__(kStressEl * 7) k_stress(const double* __restri
   const double invdet = 1.0 / (Jt0 * Jr1 - Jt1 * Jr0);
   const double R21 = rr[1] - rr[0], R31 = rr[2] - rr[0];
   const double T31 = th[2] - th[0], T21 = th[1] - th[0];
-  const double th_ip = th[0] * c_N3s[ip][0] + th[1] * c_N3s[ip][1] + th[2] * c_N3s[ip][2];
-  const double r_ip = rr[0] * c_N3s[ip][0] + rr[1] * c_N3s[ip][1] + rr[2] * c_N3s[ip][2];
-  double s, c;
-  sincos(th_ip, &s, &c);
-  const double cr = c / r_ip, sr = s / r_ip;
-  const double a11 = R31 * cr - T31 * s, a12 = -R21 * cr + T21 * s;
-  const double a21 = -R31 * sr - T31 * c, a22 = R21 * sr + T21 * c;
-  double exx = 0.0, ezz = 0.0, duxdz = 0.0, duzdx = 0.0;
+  const size_t st = (size_t)nel;
+  for (int ip = 0; ip < 7; ++ip) {
+    const double th_ip = th[0] * c_N3s[ip][0] + th[1] * c_N3s[ip][1] + th[2] * c_N3s[ip][2];
+    const double r_ip = rr[0] * c_N3s[ip][0] + rr[1] * c_N3s[ip][1] + rr[2] * c_N3s[ip][2];
+    double s, c;
+    sincos(th_ip, &s, &c);
+    const double cr = c / r_ip, sr = s / r_ip;
+    const double a11 = R31 * cr - T31 * s, a12 = -R21 * cr + T21 * s;
+    const double a21 = -R31 * sr - T31 * c, a22 = R21 * sr + T21 * c;
+    double exx = 0.0, ezz = 0.0, duxdz = 0.0, duzdx = 0.0;
 #pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    const double dx = (a11 * c_dNs[ip][0][k] + a12 * c_dNs[ip][1][k]) * invdet;
-    const double dz = (a21 * c_dNs[ip][0][k] + a22 * c_dNs[ip][1][k]) * invdet;
-    exx += dx * ux[k];
-    ezz += dz * uz[k];
-    duxdz += dz * ux[k];
-    duzdx += dx * uz[k];
+    for (int k = 0; k < 6; ++k) {
+      const double dx = (a11 * c_dNs[ip][0][k] + a12 * c_dNs[ip][1][k]) * invdet;
+      const double dz = (a21 * c_dNs[ip][0][k] + a22 * c_dNs[ip][1][k]) * invdet;
+      exx += dx * ux[k];
+      ezz += dz * uz[k];
+      duxdz += dz * ux[k];
+      duzdx += dx * uz[k];
+    }
+    const double exz = 0.5 * (duxdz + duzdx);
+    const double et = eta[(size_t)ip * st + e];
+    double txx, tzz, txz;
+    if (C) {
+      const double c11 = C[(size_t)(0 * 7 + ip) * st + e] * et, c33 = C[(size_t)(1 * 7 + ip) * st + e] * et;
+      const double c55 = C[(size_t)(2 * 7 + ip) * st + e] * et, c13 = C[(size_t)(3 * 7 + ip) * st + e] * et;
+      const double c15 = C[(size_t)(4 * 7 + ip) * st + e] * et, c35 = C[(size_t)(5 * 7 + ip) * st + e] * et;
+      const double pa = -exx / 3.0 + 2.0 * ezz / 3.0, pb = 2.0 * exx / 3.0 - ezz / 3.0;
+      txx = c13 * pa + c11 * pb + c15 * exz;
+      tzz = c33 * pa + c13 * pb + c35 * 2.0 * exz;
+      txz = c35 * pa + c15 * pb + c55 * exz;
+    } else {
+      txx = et * (4.0 / 3.0 * exx - 2.0 / 3.0 * ezz);
+      tzz = et * (-2.0 / 3.0 * exx + 4.0 / 3.0 * ezz);
+      txz = et * 2.0 * exz;
+    }
+    double* o = out + (size_t)ip * st + e;
+    const size_t blk = 7 * st;
+    o[0 * blk] = exx;
+    o[1 * blk] = ezz;
+    o[2 * blk] = exz;
+    o[3 * blk] = sqrt(0.5 * (exx * exx + ezz * ezz) + exz * exz);
+    o[4 * blk] = txx;
+    o[5 * blk] = tzz;
+    o[6 * blk] = txz;
+    o[7 * blk] = sqrt(0.5 * (txx * txx + tzz * tzz) + txz * txz);
   }
-  const double exz = 0.5 * (duxdz + duzdx);
-  double txx, tzz, txz;
-  if (C) {
-    const double c11 = cf[0], c33 = cf[1], c55 = cf[2], c13 = cf[3], c15 = cf[4], c35 = cf[5];
-    const double pa = -exx / 3.0 + 2.0 * ezz / 3.0, pb = 2.0 * exx / 3.0 - ezz / 3.0;
-    txx = c13 * pa + c11 * pb + c15 * exz;
-    tzz = c33 * pa + c13 * pb + c35 * 2.0 * exz;
-    txz = c35 * pa + c15 * pb + c55 * exz;
-  } else {
-    txx = et * (4.0 / 3.0 * exx - 2.0 / 3.0 * ezz);
-    tzz = et * (-2.0 / 3.0 * exx + 4.0 / 3.0 * ezz);
-    txz = et * 2.0 * exz;
-  }
-  double* o = out + i;
-  const size_t blk = 7 * st;
-  o[0 * blk] = exx;
-  o[1 * blk] = ezz;
-  o[2 * blk] = exz;
-  o[3 * blk] = sqrt(0.5 * (exx * exx + ezz * ezz) + exz * exz);
-  o[4 * blk] = txx;
-  o[5 * blk] = tzz;
-  o[6 * blk] = txz;
-  o[7 * blk] = sqrt(0.5 * (txx * txx + tzz * tzz) + txz * txz);
-}
-
-static void launch_k_stress(Ctx& c, const double* U, const double* eta, const double* C, double* o) {
-  const int64_t nel = c.fine.nel;
-  ++g_klaunch;
-  k_stress<<<(int)div_up(nel, kStressEl), dim3(kStressEl, 7), 0, c.stream>>>(
-      U, c.theta_lat, c.r_lat, eta, C, o, (int)nel, c.fine.ncr, (int)c.fine.A(), (int)c.fine.B());
-  DP_LAUNCH_CHECK();
 }
 
 // k_stress on the inputs staged by the last dp_stress call (kernel timing).
@@ -159,7 +140,11 @@ void launch_stress_staged(Ctx& c, bool tensor) {
   double* eta = c.stress_buf;
   double* C = eta + 7 * nel;
   double* o = C + 42 * nel;
-  launch_k_stress(c, (const double*)c.work[W_RES], eta, tensor ? C : nullptr, o);
+  ++g_klaunch;
+  k_stress<<<(int)div_up(nel, 128), 128, 0, c.stream>>>((const double*)c.work[W_RES], c.theta_lat, c.r_lat, eta,
+                                                         tensor ? C : nullptr, o, (int)nel, c.fine.ncr,
+                                                         (int)c.fine.A(), (int)c.fine.B());
+  DP_LAUNCH_CHECK();
 }
 
 }  // namespace dp
@@ -200,7 +185,10 @@ extern "C" int dp_stress(dp_ctx* h, const double* Ucart, const double* eta_ip, i
     double* ulat = (double*)c.work[W_RES];
     DP_CUDA(cudaMemcpyAsync(stage, Ucart, sizeof(double) * 2 * nn, kin, c.stream));
     launch_gather_ref2lat(c, stage, ulat, 2);
-    launch_k_stress(c, ulat, eta, C6 ? C : nullptr, o);
+    ++g_klaunch;
+    k_stress<<<(int)div_up(nel, 128), 128, 0, c.stream>>>(ulat, c.theta_lat, c.r_lat, eta, C6 ? C : nullptr, o,
+                                                           (int)nel, c.fine.ncr, (int)c.fine.A(), (int)c.fine.B());
+    DP_LAUNCH_CHECK();
     c.stress_tensor = C6 != nullptr;
     DP_CUDA(cudaMemcpyAsync(out, o, sizeof(double) * 56 * nel, kind_out(mem), c.stream));
     DP_CUDA(cudaStreamSynchronize(c.stream));

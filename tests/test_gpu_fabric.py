@@ -46,8 +46,8 @@ def test_fse_matches_oracle():
     # eigenvectors agree up to sign
     assert np.abs(np.abs(got["vx1"] * x1 + got["vy1"] * y1) - 1).max() < 1e-12
     assert np.abs(np.abs(got["vx2"] * x2 + got["vy2"] * y2) - 1).max() < 1e-12
-    und = np.zeros(F.shape[:2], dtype=bool)
-    und[::17] = True
+    und = np.all(F == np.eye(2), axis=(-2, -1))                # the undeformed IPs
+    assert und.any()
     assert np.all(got["vx1"][und] == 1.0) and np.all(got["vy1"][und] == 0.0)
 
 

@@ -44,7 +44,8 @@ def test_thermal_step_repeats_and_reports():
     with StokesContext(16, 64, "continuous") as ctx:
         a = ctx.thermal_step(T, rho, 1e6)
         b = ctx.thermal_step(T, rho, 1e6)
-        assert np.array_equal(a[0], b[0]) and a[1] == b[1]
+        # the element-by-element sums use atomics, so repeats agree to round-off, not bitwise
+        assert np.abs(a[0] - b[0]).max() / np.abs(a[0]).max() < 1e-12 and abs(a[1] - b[1]) <= 1
         with pytest.raises(Exception):
             ctx.thermal_step(T, rho, 1e6, itmax=2)            # not converged
         with pytest.raises(Exception):
