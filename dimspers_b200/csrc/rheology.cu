@@ -160,10 +160,11 @@ extern "C" int dp_viscosity_arrhenius(dp_ctx* h, const dp_arrhenius* law, const 
     if (nvert != nv) throw BadArg("P_vertex must hold the " + std::to_string(nv) + " vertex values");
     if (!(law->T0 > 0.0) || !(law->R > 0.0)) throw BadArg("T0 and R must be positive");
     static bool uploaded[64] = {false};
-    if (c.device >= 0 && c.device < 64 && !uploaded[c.device]) {
+    if (c.device < 0 || c.device >= 64 || !uploaded[c.device]) {
       upload_rheology_constants();
       upload_stress_constants();
-      uploaded[c.device] = true;
+      DP_CUDA(cudaDeviceSynchronize());  // the copies are on the default stream; ours does not wait on it
+      if (c.device >= 0 && c.device < 64) uploaded[c.device] = true;
     }
     if (!c.rheo_buf) dalloc(&c.rheo_buf, 28 * nel + 4 * nn);
     double* e2 = c.rheo_buf;

@@ -161,9 +161,10 @@ extern "C" int dp_stress(dp_ctx* h, const double* Ucart, const double* eta_ip, i
     const int64_t nel = c.fine.nel, nn = c.fine.nnod;
     if (ld_eta < nel || (C6 && ld_C < nel)) throw BadArg("leading dimension below nel");
     static bool uploaded[64] = {false};
-    if (c.device >= 0 && c.device < 64 && !uploaded[c.device]) {
+    if (c.device < 0 || c.device >= 64 || !uploaded[c.device]) {
       upload_stress_constants();
-      uploaded[c.device] = true;
+      DP_CUDA(cudaDeviceSynchronize());  // the copies are on the default stream; ours does not wait on it
+      if (c.device >= 0 && c.device < 64) uploaded[c.device] = true;
     }
     if (!c.stress_buf) dalloc(&c.stress_buf, (7 + 42 + 56) * nel);
     double* eta = c.stress_buf;

@@ -344,11 +344,12 @@ extern "C" int dp_thermal_step(dp_ctx* h, const dp_thermal_opts* o, const double
     const Level& L = c.fine;
     const int64_t nel = L.nel, nn = L.nnod;
     static bool uploaded[64] = {false};
-    if (c.device >= 0 && c.device < 64 && !uploaded[c.device]) {
+    if (c.device < 0 || c.device >= 64 || !uploaded[c.device]) {
       upload_stress_constants();
       upload_rheology_constants();
       upload_thermal_constants();
-      uploaded[c.device] = true;
+      DP_CUDA(cudaDeviceSynchronize());  // the copies are on the default stream; ours does not wait on it
+      if (c.device >= 0 && c.device < 64) uploaded[c.device] = true;
     }
     if (!c.th_buf) dalloc(&c.th_buf, kThPack * nel + TV_COUNT * nn);
     const int heated = o->heated ? 1 : 0;
@@ -390,9 +391,16 @@ extern "C" int dp_thermal_step(dp_ctx* h, const dp_thermal_opts* o, const double
       ensure_ctl(c);  // the capture streams of loop bodies
       cudaGraph_t g = nullptr;
       DP_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed));
-      {
+      try {
         PdlScope pdl(1);
         th_emit_loop(c, heated);
+      } catch (...) {
+        // leave the stream out of capture mode before reporting the error
+        cudaGraph_t partial = nullptr;
+        cudaStreamEndCapture(c.stream, &partial);
+        if (partial) cudaGraphDestroy(partial);
+        cudaGetLastError();
+        throw;
       }
       DP_CUDA(cudaStreamEndCapture(c.stream, &g));
       cudaGraphExec_t ex = nullptr;
