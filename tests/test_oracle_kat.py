@@ -291,3 +291,26 @@ def test_thermal_long_step_converges_to_conduction_profile():
         exact = 4000.0 + (300.0 - 4000.0) * np.log(gr.r / 1.22) / np.log(2.22 / 1.22)
         errs.append(np.abs(T - exact).max())
     assert errs[1] < errs[0] / 6 and errs[1] < 0.05
+
+
+@pytest.mark.parametrize("pressure", ["continuous", "discontinuous"])
+def test_hydrostatic_balance_converges(pressure):
+    """A manufactured solution the radial buoyancy force admits: uniform rho
+    and eta give u = 0 and p = g rho r + const.  The discrete velocity vanishes
+    and the pressure is linear in r, both to high order under refinement (the
+    curved geometry makes neither exact)."""
+    errs = []
+    for nr, nt in ((4, 32), (8, 64)):
+        prob = OS.make_problem(nr, nt, pressure)
+        gr = prob.gr
+        nel = prob.th.shape[1]
+        out = OS.solve_stokes(prob, np.ones((nel, 7)), np.full(gr.nnod, 2.0), 1.5, rtol=1e-12, itmax=2000)
+        U, P = out["U"], out["P"]
+        rp = np.zeros(len(P))
+        rp[prob.e2nP] = gr.r[gr.e2n[:3]]
+        A = np.vstack([rp, np.ones(len(P))]).T
+        coef = np.linalg.lstsq(A, P, rcond=None)[0]
+        errs.append((np.abs(U).max(), np.abs(P - A @ coef).max()))
+        assert abs(coef[0] - 3.0) < 1e-5                        # dp/dr = g rho
+    assert errs[1][0] < errs[0][0] / 15 and errs[1][0] < 1e-9
+    assert errs[1][1] < errs[0][1] / 10 and errs[1][1] < 1e-6
