@@ -76,7 +76,7 @@ def test_bad_arguments_are_reported():
         build_mesh(4, 2)
 
 
-def test_sizes_match_survey_table():
+def test_sizes_match_the_split1_formulas():
     for (ncr, nct), (nel, nnod, npd) in {(32, 256): (16384, 33280, 49152),
                                          (128, 1024): (262144, 526336, 786432)}.items():
         d = _lib.MeshDesc(ncr, nct, 1.22, 2.22, 1, 0, 1)
