@@ -20,8 +20,12 @@ Follows the reference's threaded path, the one MAIN.jl calls (:272-291):
   heated_bottom (src/Setup/boundary_conditions.jl:77-93): T fixed to Ttop on
       the outer wall and Tbot on the inner one; insulated_bottom (:95-): the
       outer wall only.
-Here the linear system is solved directly (SuperLU): the GPU's PCG and the
-reference's GMRES both stop at a relative residual of sqrt(eps).
+The linear system is solved directly (SuperLU) by default; solver="gmres"
+restates the reference's call instead: Krylov.jl's gmres with its defaults
+(restart = false, i.e. full GMRES; atol = rtol = sqrt(eps); itmax = 2n; no
+preconditioner), modified Gram-Schmidt Arnoldi with Givens rotations, stopping
+when the residual norm falls to atol + rtol ||b||.  The GPU's PCG stops at the
+same test.
 """
 import numpy as np
 import scipy.sparse as sp
@@ -83,7 +87,54 @@ def boundary(gr, Ttop, Tbot, heated=True):
     return np.concatenate(nodes), np.concatenate(vals)
 
 
-def thermal_step(gr, th, r, T, rho_node, K, Cp, dt, fixed, tfix):
+def gmres(A, b, atol=np.sqrt(np.finfo(float).eps), rtol=np.sqrt(np.finfo(float).eps), itmax=None):
+    """Full GMRES from x0 = 0 (Krylov.jl gmres defaults); returns (x, iterations, ||r||)."""
+    n = b.size
+    itmax = 2 * n if itmax is None else itmax
+    beta = np.linalg.norm(b)
+    eps = atol + rtol * beta
+    if beta <= eps:
+        return np.zeros(n), 0, beta
+    V = [b / beta]
+    H = []                                   # columns of the Hessenberg matrix after the rotations
+    cs, sn = [], []
+    g = [beta]
+    k = 0
+    rnorm = beta
+    while rnorm > eps and k < itmax:
+        w = A @ V[k]
+        h = np.zeros(k + 2)
+        for i in range(k + 1):               # modified Gram-Schmidt
+            h[i] = V[i] @ w
+            w = w - h[i] * V[i]
+        h[k + 1] = wn = np.linalg.norm(w)
+        for i in range(k):                   # previous rotations
+            t = cs[i] * h[i] + sn[i] * h[i + 1]
+            h[i + 1] = -sn[i] * h[i] + cs[i] * h[i + 1]
+            h[i] = t
+        d = np.hypot(h[k], h[k + 1])
+        c, s = h[k] / d, h[k + 1] / d
+        cs.append(c)
+        sn.append(s)
+        h[k] = d
+        h[k + 1] = 0.0
+        g.append(-s * g[k])
+        g[k] = c * g[k]
+        H.append(h[:k + 1].copy())
+        rnorm = abs(g[k + 1])
+        k += 1
+        if wn == 0.0:                        # lucky breakdown: the Krylov space holds the solution
+            break
+        V.append(w / wn)
+    R = np.zeros((k, k))
+    for j in range(k):
+        R[:j + 1, j] = H[j]
+    y = np.linalg.solve(np.triu(R), np.array(g[:k]))
+    x = np.column_stack(V[:k]) @ y
+    return x, k, rnorm
+
+
+def thermal_step(gr, th, r, T, rho_node, K, Cp, dt, fixed, tfix, solver="direct"):
     """One solveDiffusion_threaded step: returns the new nodal T."""
     Ke, Me = element_matrices(th, r, rho_node, gr.e2n, K, Cp)
     MT = _global(gr.e2n, Me, gr.nnod)
@@ -94,5 +145,9 @@ def thermal_step(gr, th, r, T, rho_node, K, Cp, dt, fixed, tfix):
     Tn[fixed] = tfix
     F = F - A[:, fixed] @ tfix
     free = np.setdiff1d(np.arange(gr.nnod), fixed)
-    Tn[free] = spla.spsolve(A[free][:, free].tocsc(), F[free])
+    Aff = A[free][:, free].tocsc()
+    if solver == "gmres":
+        Tn[free] = gmres(Aff.tocsr(), F[free])[0]
+    else:
+        Tn[free] = spla.spsolve(Aff, F[free])
     return Tn

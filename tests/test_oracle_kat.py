@@ -314,3 +314,32 @@ def test_hydrostatic_balance_converges(pressure):
         assert abs(coef[0] - 3.0) < 1e-5                        # dp/dr = g rho
     assert errs[1][0] < errs[0][0] / 15 and errs[1][0] < 1e-9
     assert errs[1][1] < errs[0][1] / 10 and errs[1][1] < 1e-6
+
+
+def test_thermal_gmres_restatement_meets_its_stopping_test():
+    """The reference's solve (Krylov.jl gmres, full, sqrt(eps) tolerances)
+    restated: it stops at ||r|| <= atol + rtol ||b|| with the true residual
+    there too, and agrees with the direct solve to kappa * sqrt(eps)."""
+    from oracle import thermal as OT
+    prob = OS.make_problem(4, 32, "continuous")
+    gr = prob.gr
+    rng = np.random.default_rng(8)
+    Ke, Me = OT.element_matrices(prob.th, prob.r, 1.0 + 0.1 * rng.random(gr.nnod), gr.e2n, 1.0, 1.0)
+    A = OT._global(gr.e2n, Me + 1e-3 * Ke, gr.nnod)
+    b = rng.standard_normal(gr.nnod)
+    x, it, rn = OT.gmres(A, b)
+    eps = np.sqrt(np.finfo(float).eps) * (1.0 + np.linalg.norm(b))
+    assert 0 < it < gr.nnod and rn <= eps
+    assert np.linalg.norm(b - A @ x) <= 1.01 * eps
+    xd = spla_solve(A, b)
+    assert np.abs(x - xd).max() / np.abs(xd).max() < 1e-5
+    fixed, tfix = OT.boundary(gr, 300.0, 4000.0)
+    T0 = np.full(gr.nnod, 1000.0)
+    Tg = OT.thermal_step(gr, prob.th, prob.r, T0, np.ones(gr.nnod), 1.0, 1.0, 1e-2, fixed, tfix, solver="gmres")
+    Td = OT.thermal_step(gr, prob.th, prob.r, T0, np.ones(gr.nnod), 1.0, 1.0, 1e-2, fixed, tfix)
+    assert np.abs(Tg - Td).max() / np.abs(Td).max() < 1e-6
+
+
+def spla_solve(A, b):
+    import scipy.sparse.linalg as spla
+    return spla.spsolve(A.tocsc(), b)
