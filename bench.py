@@ -68,6 +68,11 @@ def parse():
     ap.add_argument("--no-guess", action="store_true", help="fast arm without the learned initial guess")
     ap.add_argument("--profile-apply", action="store_true",
                     help="assemble the workload and launch the fine-level FP32 A-apply 3 times (for ncu)")
+    ap.add_argument("--postprocess", action="store_true",
+                    help="the kernels around the solve (stress, viscosity, DEM tensor, thermal step) on the GPU "
+                         "beside the oracle's CPU restatements, one JSON line each")
+    ap.add_argument("--dem-sample", type=int, default=4096,
+                    help="elements in the CPU sample of the DEM tensor lookup (scaled to the mesh)")
     return ap.parse_args()
 
 
@@ -448,9 +453,6 @@ def run_reference(args, rank, world):
         return
     n_outer = reference_outer_iterations(args)
     t_setup, t_iter = cpu_sample(args, n_outer, args.cpu_iters)
-    steps = []
-    for _ in range(args.warmup):
-        pass
     per_solve = t_setup + n_outer * t_iter
     value = 1.0 / per_solve
     line = {
@@ -465,6 +467,80 @@ def run_reference(args, rank, world):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------ kernels around the solve ----
+def cpu_postprocess(args):
+    """The oracle's CPU restatements on the inputs the GPU timing uses: ms per
+    call (best of 2), on one thread (BLAS pools limited to 1).  The DEM
+    lookup's per-IP Python loop is timed on the first --dem-sample elements
+    and scaled to the mesh."""
+    from threadpoolctl import threadpool_limits
+    with threadpool_limits(1):
+        return _cpu_postprocess(args)
+
+
+def _cpu_postprocess(args):
+    import numpy as np
+    import oracle.fabric as OF
+    import oracle.rheology as RH
+    import oracle.solver as OS
+    import oracle.stress as ST
+    import oracle.thermal as OT
+    from dimspers_b200 import inputs, kernel_times as KT
+
+    def best(fn, reps=2):
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t0)
+        return 1e3 * min(ts)
+
+    nr, nt = args.nr, args.nt
+    out = {}
+    prob = OS.make_problem(nr, nt, "discontinuous")
+    gr = prob.gr
+
+    class MV:
+        theta, r, e2n, th_el, r_el = gr.theta, gr.r, gr.e2n, prob.th, prob.r
+        nel, nnod = gr.e2n.shape[1], gr.nnod
+
+    m = inputs.make_material(MV, "aniso", seed=1)
+    rng = np.random.default_rng(0)
+    U = rng.standard_normal(2 * gr.nnod)
+    out["k_stress"] = (best(lambda: ST.stress(U, m.eta_ip, prob.th, prob.r, gr.e2n, m.C6)), "whole mesh")
+    T, P, r, eps, tau, coh = KT.inputs_viscosity(MV, nr, nt, rng)
+    eta0 = np.full((MV.nel, 7), 3.3e21)
+    out["k_viscosity_arrhenius"] = (best(lambda: RH.arrhenius_viscosity(
+        eta0, T, P, r, gr.e2n, eps, tau, coh, 5e20, 8.314, 100e3, 1e-6, 1600.0, 30.0)), "whole mesh")
+    d = np.load(KT.DEM_FIXTURE)
+    tab = OF.dem_tables(d["C"], d["ax"])
+    x1, y1, r1, r2 = KT.inputs_dem(MV.nel, rng)
+    ns = min(args.dem_sample, MV.nel)
+    ms = best(lambda: OF.anisotropic_tensor(x1[:ns], y1[:ns], r1[:ns], r2[:ns], tab, 0.02), reps=1)
+    out["k_dem_tensor"] = (ms * MV.nel / ns, f"{ns} elements, scaled to {MV.nel}")
+    pc = OS.make_problem(nr, nt, "continuous")
+    T, rho, dt = KT.inputs_thermal(pc.gr, nr, np.random.default_rng(0))
+    fixed, tfix = OT.boundary(pc.gr, 300.0, 4000.0)
+    out["k_th_apply"] = (best(lambda: OT.thermal_step(pc.gr, pc.th, pc.r, T, rho, 3.3, 1.2e3, dt, fixed, tfix,
+                                                      solver="gmres"), reps=1),
+                         "whole step: assembly + the reference's full GMRES")
+    return out
+
+
+def postprocess(args):
+    import torch
+    size = f"{args.nr}x{args.nt}"
+    gpu = {}
+    if torch.cuda.is_available():
+        from dimspers_b200 import kernel_times
+        gpu = {rec["kernel"]: rec for rec in kernel_times.measure([size])}
+    cpu = cpu_postprocess(args)
+    for k, (ms, sample) in cpu.items():
+        line = {"postprocess": k, "size": size, "gpu": gpu.get(k),
+                "cpu_baseline": {"value": ms, "unit": "ms per call", "cores": 1, "kind": "port", "sample": sample}}
+        print(json.dumps(line), flush=True)
 
 
 def reference_outer_iterations(args):
@@ -486,6 +562,10 @@ def main():
         return
     if args.profile_apply:
         profile_apply(args)
+        return
+    if args.postprocess:
+        if rank == 0:
+            postprocess(args)
         return
     if args.impl == "reference":
         run_reference(args, rank, world)
