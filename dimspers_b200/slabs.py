@@ -157,3 +157,61 @@ def distributed_pcg(part, apply_local, b, diag, free, rtol, atol, itmax, ncomp=1
         rz = rz_new
         it += 1
     return x, it, float(torch.sqrt(rr))
+
+
+def distributed_stokes_pcg(part, apply_K, diag_K, free_u, apply_G, apply_GT, pc_S, rhs_u, n_p_global,
+                           rtol=1e-8, itmax=200, itmin=10, inner_rtol=1e-12, inner_itmax=20000):
+    """StokesPcCG (IterativeSolvers.jl:94-168) on slab-local data, for a
+    pressure space whose DOFs belong to one element (discontinuous P1): the
+    Schur PCG on S = G^T K^-1 G with the same step order, Polak-Ribiere beta,
+    mean removal and stopping test as the single-GPU solve, an inner
+    Jacobi-PCG on K for each K^-1, and only these crossing ranks: the
+    velocity exchange after each K or G apply and all-reduces for dots, sums
+    and the stopping test.
+
+    apply_K(u) / apply_G(p): the slab's partial element sums (exchanged here);
+    apply_GT(u) -> the slab's pressure vector (element-local, u consistent);
+    pc_S(r): the Schur preconditioner on the slab's pressure DOFs; diag_K and
+    rhs_u: assembled (exchanged) local vectors; free_u: local mask of the free
+    velocity DOFs.  Returns (U, P, outer iterations, relative residual)."""
+    def psum(v):
+        s = torch.sum(v).reshape(1)
+        if part.world > 1:
+            dist.all_reduce(s)
+        return s[0]
+
+    def pdot(a, b):
+        return psum(a * b)
+
+    def rm0(a):                                   # rm0space! (IterativeSolvers.jl:172-186)
+        return a - psum(a) / n_p_global
+
+    def inner(b):
+        return distributed_pcg(part, apply_K, b, diag_K, free_u, inner_rtol, 0.0, inner_itmax, ncomp=2)[0]
+
+    U = inner(rhs_u)
+    r = rm0(-apply_GT(U))
+    P = torch.zeros_like(r)
+    r0 = torch.sqrt(pdot(r, r))
+    tol = r0 * rtol
+    d = pc_S(r)
+    q = d.clone()
+    it = 0
+    nr = r0
+    for it in range(1, itmax + 1):
+        q = rm0(q)
+        rd = pdot(r, d)
+        z = inner(part.exchange_add(apply_G(q), 2))
+        Sq = apply_GT(z)
+        alpha = rd / pdot(q, Sq)
+        rlast = r
+        P = P + alpha * q
+        U = U + alpha * z
+        r = rm0(r - alpha * Sq)
+        nr = torch.sqrt(pdot(r, r))
+        if nr < tol and it >= itmin:
+            break
+        d = pc_S(r)
+        beta = pdot(r - rlast, d) / rd
+        q = d + beta * q
+    return U, P, it, float(nr / r0) if r0 > 0 else 0.0
