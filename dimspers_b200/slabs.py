@@ -159,38 +159,79 @@ def distributed_pcg(part, apply_local, b, diag, free, rtol, atol, itmax, ncomp=1
     return x, it, float(torch.sqrt(rr))
 
 
-def distributed_stokes_pcg(part, apply_K, diag_K, free_u, apply_G, apply_GT, pc_S, rhs_u, n_p_global,
-                           rtol=1e-8, itmax=200, itmin=10, inner_rtol=1e-12, inner_itmax=20000):
-    """StokesPcCG (IterativeSolvers.jl:94-168) on slab-local data, for a
-    pressure space whose DOFs belong to one element (discontinuous P1): the
-    Schur PCG on S = G^T K^-1 G with the same step order, Polak-Ribiere beta,
-    mean removal and stopping test as the single-GPU solve, an inner
-    Jacobi-PCG on K for each K^-1, and only these crossing ranks: the
-    velocity exchange after each K or G apply and all-reduces for dots, sums
-    and the stopping test.
+class ElementPressure:
+    """Discontinuous P1: every pressure DOF belongs to one element, so a slab's
+    pressure vector (3 per local element) needs no exchange; sums all-reduce."""
 
-    apply_K(u) / apply_G(p): the slab's partial element sums (exchanged here);
-    apply_GT(u) -> the slab's pressure vector (element-local, u consistent);
-    pc_S(r): the Schur preconditioner on the slab's pressure DOFs; diag_K and
-    rhs_u: assembled (exchanged) local vectors; free_u: local mask of the free
-    velocity DOFs.  Returns (U, P, outer iterations, relative residual)."""
-    def psum(v):
+    def __init__(self, part, n_global):
+        self.part, self.n_global = part, n_global
+
+    def sum(self, v):
         s = torch.sum(v).reshape(1)
-        if part.world > 1:
+        if self.part.world > 1:
             dist.all_reduce(s)
         return s[0]
 
-    def pdot(a, b):
-        return psum(a * b)
+    def complete(self, v):
+        return v
 
-    def rm0(a):                                   # rm0space! (IterativeSolvers.jl:172-186)
-        return a - psum(a) / n_p_global
+    def remove_mean(self, a):
+        return a - self.sum(a) / self.n_global
+
+
+class VertexPressure:
+    """Continuous P1: pressure on the P2 lattice's vertex nodes (even a and b),
+    held as a slab-lattice vector that is zero elsewhere; the shared columns
+    are vertex columns, completed by the same exchange as the velocity and
+    counted once in sums."""
+
+    def __init__(self, part):
+        self.part = part
+        gn = part.global_nodes()
+        a, b = gn % part.A, gn // part.A
+        vert = (a % 2 == 0) & (b % 2 == 0)
+        self.mask = torch.as_tensor(vert)
+        self.owned = torch.as_tensor(vert & part.owned())
+        self.n_global = (part.ncr + 1) * part.nct
+
+    def sum(self, v):
+        s = torch.sum(torch.where(self.owned, v, torch.zeros_like(v))).reshape(1)
+        if self.part.world > 1:
+            dist.all_reduce(s)
+        return s[0]
+
+    def complete(self, v):
+        return self.part.exchange_add(v, 1)
+
+    def remove_mean(self, a):
+        return torch.where(self.mask, a - self.sum(a) / self.n_global, a)
+
+
+def distributed_stokes_pcg(part, apply_K, diag_K, free_u, apply_G, apply_GT, pc_S, rhs_u, pspace,
+                           rtol=1e-8, itmax=200, itmin=10, inner_rtol=1e-12, inner_itmax=20000):
+    """StokesPcCG (IterativeSolvers.jl:94-168) on slab-local data: the Schur
+    PCG on S = G^T K^-1 G with the same step order, Polak-Ribiere beta, mean
+    removal and stopping test as the single-GPU solve, an inner Jacobi-PCG on
+    K for each K^-1, and only these crossing ranks: the velocity exchange
+    after each K or G apply, the pressure exchange after each G^T apply
+    (continuous pressure only), and all-reduces for dots, sums and the
+    stopping test.
+
+    apply_K(u) / apply_G(p) / apply_GT(u): the slab's partial element sums
+    (completed here); pc_S(r): the Schur preconditioner on the slab's
+    pressure DOFs; diag_K and rhs_u: assembled (exchanged) local vectors;
+    free_u: local mask of the free velocity DOFs; pspace: ElementPressure or
+    VertexPressure.  Returns (U, P, outer iterations, relative residual)."""
+    def pdot(a, b):
+        return pspace.sum(a * b)
+
+    rm0 = pspace.remove_mean                      # rm0space! (IterativeSolvers.jl:172-186)
 
     def inner(b):
         return distributed_pcg(part, apply_K, b, diag_K, free_u, inner_rtol, 0.0, inner_itmax, ncomp=2)[0]
 
     U = inner(rhs_u)
-    r = rm0(-apply_GT(U))
+    r = rm0(-pspace.complete(apply_GT(U)))
     P = torch.zeros_like(r)
     r0 = torch.sqrt(pdot(r, r))
     tol = r0 * rtol
@@ -202,7 +243,7 @@ def distributed_stokes_pcg(part, apply_K, diag_K, free_u, apply_G, apply_GT, pc_
         q = rm0(q)
         rd = pdot(r, d)
         z = inner(part.exchange_add(apply_G(q), 2))
-        Sq = apply_GT(z)
+        Sq = pspace.complete(apply_GT(z))
         alpha = rd / pdot(q, Sq)
         rlast = r
         P = P + alpha * q
