@@ -250,11 +250,12 @@ class StokesContext:
                                                _ptr(eta), DP_MEM_HOST))
         return np.array(eta)
 
-    def thermal_step(self, T, rho_node, dt, **opts):
+    def thermal_step(self, T, rho_node, dt, raise_on_status=True, **opts):
         """solveDiffusion_threaded (AssemblerThermal.jl:1-57): one backward-Euler
         step of the nodal temperature T (reference numbering).  opts: K, Cp,
         Ttop, Tbot, heated, rtol, atol, itmax (defaults: dp_default_thermal_opts).
-        Returns (T_new, iterations, relres)."""
+        Returns (T_new, iterations, relres); with raise_on_status=False a step
+        that stopped at itmax (DP_NOT_CONVERGED) returns its last iterate."""
         o = _lib.ThermalOpts()
         lib().dp_default_thermal_opts(C.byref(o))
         o.dt = float(dt)
@@ -268,8 +269,9 @@ class StokesContext:
             raise ValueError("T and rho_node must hold nnod values")
         it = C.c_int32(0)
         rel = C.c_double(0.0)
-        self._chk(lib().dp_thermal_step(self.h, C.byref(o), _ptr(rho), _ptr(Tn), C.byref(it), C.byref(rel),
-                                        DP_MEM_HOST))
+        st = lib().dp_thermal_step(self.h, C.byref(o), _ptr(rho), _ptr(Tn), C.byref(it), C.byref(rel), DP_MEM_HOST)
+        if st != 0 and (raise_on_status or st >= 2):
+            self._chk(st)
         return Tn, it.value, rel.value
 
     def fse(self, F):
