@@ -187,10 +187,11 @@ def traffic_from_profiles(nr, nt):
 
 def start_cpu_sample(args):
     """The CPU oracle sample runs in its own process, concurrently with the GPU
-    timing (it needs one host core; the GPU path needs one more)."""
+    timing, on one host thread (the GPU path needs one more)."""
     cmd = [sys.executable, os.path.abspath(__file__), "--cpu-sample-only", "--nr", str(args.nr), "--nt", str(args.nt),
            "--pressure", args.pressure, "--kind", args.kind, "--cpu-iters", str(args.cpu_iters)]
-    return subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1", MKL_NUM_THREADS="1")
+    return subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, env=env)
 
 
 def finish_cpu_sample(proc, args, n_outer):
@@ -201,7 +202,8 @@ def finish_cpu_sample(proc, args, n_outer):
         return {"value": None, "unit": UNIT, "cores": 1, "kind": "port", "sample": f"failed: {e}"}
     per_solve = d["t_setup"] + n_outer * d["t_iter"]
     return {"value": 1.0 / per_solve, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"FP64 NumPy/SciPy oracle: assembly + SuperLU factorisation ({d['t_setup']:.1f} s) + "
+            "sample": f"FP64 oracle on one thread: C element blocks, SciPy assembly + SuperLU factorisation "
+                      f"({d['t_setup']:.1f} s) + "
                       f"{args.cpu_iters} outer iterations ({d['t_iter']:.2f} s each) of the {args.nr}x{args.nt} "
                       f"workload, extrapolated to {n_outer} outer iterations (lumped-mass StokesPcCG)"}
 
@@ -410,6 +412,7 @@ def cpu_sample(args, n_outer, iters):
     outer iteration)."""
     import numpy as np
     import scipy.sparse.linalg as spla
+    import oracle.c_elements as OC
     import oracle.solver as OS
     from dimspers_b200 import inputs
 
@@ -420,7 +423,7 @@ def cpu_sample(args, n_outer, iters):
 
     mat = inputs.make_material(MV, args.kind, seed=1)
     t0 = time.perf_counter()
-    A = OS.assemble(prob, mat.eta_ip, mat.rho, mat.g, mat.C6)
+    A = OS.assemble(prob, mat.eta_ip, mat.rho, mat.g, mat.C6, elements=OC.element_matrices)
     Kf = A["KK"][prob.ifree][:, prob.ifree].tocsc()
     lu = spla.splu(Kf, permc_spec="MMD_AT_PLUS_A")
     t1 = time.perf_counter()
@@ -461,9 +464,11 @@ def run_reference(args, rank, world):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
         "config": {"workload": f"annulus {args.nr}x{args.nt} cells, {args.pressure} P1 pressure, {args.kind}",
                    "nr_cells": args.nr, "ntheta_cells": args.nt},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-                         "sample": f"assembly + SuperLU ({t_setup:.1f} s) + {args.cpu_iters} outer iterations "
-                                   f"({t_iter:.2f} s each), extrapolated to {n_outer} outer iterations"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"element blocks on {os.cpu_count()} threads (C/OpenMP restatement), sparse "
+                                   f"assembly + rotation + SuperLU factorisation (single-threaded) ({t_setup:.1f} s) + "
+                                   f"{args.cpu_iters} outer iterations ({t_iter:.2f} s each), extrapolated to "
+                                   f"{n_outer} outer iterations"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

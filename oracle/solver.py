@@ -144,10 +144,12 @@ def make_problem(ncr, nctheta, pressure="discontinuous", literal=False, pin_rota
                          omega=omega, ifree=ifree)
 
 
-def assemble(prob, eta_ip, rho_node, g, C6=None):
-    """assembly_stokes_cylindric + _prepare_matrices + _apply_bcs (vfix = 0)."""
+def assemble(prob, eta_ip, rho_node, g, C6=None, elements=None):
+    """assembly_stokes_cylindric + _prepare_matrices + _apply_bcs (vfix = 0).
+    elements: the element-block restatement to use (default the NumPy one;
+    oracle.c_elements.element_matrices is the threaded C one)."""
     gr = prob.gr
-    Ke, Ge, Me, Fb = element_matrices(prob.th, prob.r, eta_ip, rho_node, gr.e2n, g, C6)
+    Ke, Ge, Me, Fb = (elements or element_matrices)(prob.th, prob.r, eta_ip, rho_node, gr.e2n, g, C6)
     KK, GG, MM, F = global_matrices(gr.e2n, prob.e2nP, Ke, Ge, Me, Fb, gr.nnod, prob.npres)
     TT = rotation_matrix(gr.theta)
     KK, GG, F = prepare_matrices(KK, GG, F, TT)

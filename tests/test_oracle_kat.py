@@ -343,3 +343,18 @@ def test_thermal_gmres_restatement_meets_its_stopping_test():
 def spla_solve(A, b):
     import scipy.sparse.linalg as spla
     return spla.spsolve(A.tocsc(), b)
+
+
+@pytest.mark.parametrize("kind", ["iso", "aniso"])
+def test_c_and_numpy_element_restatements_agree(kind):
+    """Two independent restatements of the Stokes element blocks (NumPy,
+    oracle/assembly.py; plain C with OpenMP, oracle/stokes_elements.c) agree
+    to round-off on every packed entry."""
+    from oracle import c_elements as OC
+    prob = OS.make_problem(8, 64, "discontinuous")
+    mat = inputs.make_material(MeshView(prob), kind, seed=9)
+    ref = OA.element_matrices(prob.th, prob.r, mat.eta_ip, mat.rho, prob.gr.e2n, mat.g, mat.C6)
+    got = OC.element_matrices(prob.th, prob.r, mat.eta_ip, mat.rho, prob.gr.e2n, mat.g, mat.C6)
+    for a, b in zip(got, ref):
+        assert a.shape == b.shape
+        assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()
