@@ -71,8 +71,6 @@ def parse():
     ap.add_argument("--postprocess", action="store_true",
                     help="the kernels around the solve (stress, viscosity, DEM tensor, thermal step) on the GPU "
                          "beside the oracle's CPU restatements, one JSON line each")
-    ap.add_argument("--dem-sample", type=int, default=4096,
-                    help="elements in the CPU sample of the DEM tensor lookup (scaled to the mesh)")
     return ap.parse_args()
 
 
@@ -477,9 +475,8 @@ def run_reference(args, rank, world):
 # ------------------------------------------------ kernels around the solve ----
 def cpu_postprocess(args):
     """The oracle's CPU restatements on the inputs the GPU timing uses: ms per
-    call (best of 2), on one thread (BLAS pools limited to 1).  The DEM
-    lookup's per-IP Python loop is timed on the first --dem-sample elements
-    and scaled to the mesh."""
+    call (best of 2), on one thread (BLAS pools limited to 1; the DEM lookup
+    is the plain-C restatement run on one OpenMP thread)."""
     from threadpoolctl import threadpool_limits
     with threadpool_limits(1):
         return _cpu_postprocess(args)
@@ -487,6 +484,7 @@ def cpu_postprocess(args):
 
 def _cpu_postprocess(args):
     import numpy as np
+    import oracle.c_elements as OC
     import oracle.fabric as OF
     import oracle.rheology as RH
     import oracle.solver as OS
@@ -522,9 +520,8 @@ def _cpu_postprocess(args):
     d = np.load(KT.DEM_FIXTURE)
     tab = OF.dem_tables(d["C"], d["ax"])
     x1, y1, r1, r2 = KT.inputs_dem(MV.nel, rng)
-    ns = min(args.dem_sample, MV.nel)
-    ms = best(lambda: OF.anisotropic_tensor(x1[:ns], y1[:ns], r1[:ns], r2[:ns], tab, 0.02), reps=1)
-    out["k_dem_tensor"] = (ms * MV.nel / ns, f"{ns} elements, scaled to {MV.nel}")
+    out["k_dem_tensor"] = (best(lambda: OC.anisotropic_tensor(x1, y1, r1, r2, tab, 0.02, nthreads=1)),
+                           "whole mesh (plain C, one thread)")
     pc = OS.make_problem(nr, nt, "continuous")
     T, rho, dt = KT.inputs_thermal(pc.gr, nr, np.random.default_rng(0))
     fixed, tfix = OT.boundary(pc.gr, 300.0, 4000.0)

@@ -358,3 +358,21 @@ def test_c_and_numpy_element_restatements_agree(kind):
     for a, b in zip(got, ref):
         assert a.shape == b.shape
         assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()
+
+
+def test_c_and_python_dem_lookups_agree():
+    """The DEM tensor lookup restated twice (per-IP Python loop,
+    oracle/fabric.py; plain C, oracle/fabric_lookup.c) on the reference's
+    table: the same rows everywhere, round-off in the rotation only."""
+    from oracle import c_elements as OC
+    from oracle import fabric as OF
+    C6, ax = _dem_fixture()
+    t = OF.dem_tables(C6, ax)
+    rng = np.random.default_rng(4)
+    nel = 300
+    ang = rng.uniform(-np.pi, np.pi, (nel, 6))
+    args = (np.cos(ang), np.sin(ang), rng.uniform(-0.3, 2.0, (nel, 6)), rng.uniform(-0.3, 2.3, (nel, 6)))
+    ref = OF.anisotropic_tensor(*args, t, 0.02)
+    got = OC.anisotropic_tensor(*args, t, 0.02)
+    for a, b in zip(got, ref):
+        assert np.abs(a - b).max() < 1e-14
