@@ -1,4 +1,5 @@
-"""6-point triangle quadrature and P2 / P1 shape functions (FP64 restatement).
+"""6-point triangle quadrature and P2 / P1 shape functions (FP64 restatement;
+test infrastructure).
 
 Follows src/Algebra/Quadrature.jl:
   ip_triangle6      :80-107   (weights carry the x0.5 reference-triangle area)
