@@ -384,6 +384,14 @@ def run_ours(args, rank, world, local):
         "gpu_launches": int(sum(r["kernel_launches"] for r in reps32)),
         "roofline": roofline, "clocks": clocks,
     }
+    try:   # the whole solve against the HBM roofline, from a per-kernel byte model
+        sb = solve_bytes_model(args.nr, args.nt, last["iterations"], last["inner_iterations"], args.pressure,
+                               FAST["cheb_degree"])
+        sgbs = sb / (ms_per_step * 1e-3) / 1e9
+        line["solve_model"] = {"bytes_per_solve": sb, "achieved": sgbs, "unit": "GB/s", "frac": sgbs / pk,
+                               "note": "algorithmic bytes of every kernel of one fast solve (bench.solve_bytes_model)"}
+    except Exception as e:  # a model must never cost the measured line
+        line["solve_model"] = {"error": str(e)}
     if cpu_proc is not None:
         line["cpu_baseline"] = finish_cpu_sample(cpu_proc, args, fp64["outer_iterations"] if fp64 else
                                                  last["iterations"])
@@ -393,6 +401,41 @@ def run_ours(args, rank, world, local):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def solve_bytes_model(nr, nt, outer, inner, pressure="discontinuous", cheb_degree=3, coarse_max=1536):
+    """Algorithmic HBM bytes of one fast-path solve (FP64 Krylov, FP32 multigrid
+    V-cycle per inner iteration): every kernel's reads and writes once, from
+    the measured iteration counts.  Per-kernel figures (the kernel table):
+    FP32 apply 312 B/element + 16 B/node; FP64 apply 624 B/element + 48 B/node;
+    Chebyshev vector step 76 B/node; restriction 16 B/fine node + 40 B/coarse
+    node; prolongation 24 B/fine node; dense coarsest n^2 x 8 B; inner PCG
+    vector passes 128 B/DOF; outer: G and G^T 288 B/element + vectors, the
+    fused Schur update (5 N_P + 2 N_U) x 8 B and its dots; assembly and
+    set-up excluded."""
+    levels = []
+    r_, t_ = nr, nt
+    while True:
+        nel, nnod = 2 * r_ * t_, (2 * r_ + 1) * 2 * t_
+        levels.append((nel, nnod))
+        if 2 * nnod <= coarse_max or r_ % 2 or t_ % 2:
+            break
+        r_, t_ = r_ // 2, t_ // 2
+    vcycle = 0.0
+    for i, (nel, nnod) in enumerate(levels):
+        if i == len(levels) - 1:
+            vcycle += (2 * nnod) ** 2 * 8.0
+            break
+        cn = levels[i + 1][1]
+        vcycle += 2 * cheb_degree * (312.0 * nel + 16.0 * nnod)          # smoothing and residual applies
+        vcycle += 2 * cheb_degree * 76.0 * nnod                          # Chebyshev vector steps
+        vcycle += 16.0 * nnod + 40.0 * cn + 24.0 * nnod                  # restriction, prolongation
+    nel, nnod = levels[0]
+    n_u = 2 * nnod
+    n_p = 3 * nel if pressure == "discontinuous" else (nr + 1) * nt
+    per_inner = vcycle + 624.0 * nel + 48.0 * nnod + 128.0 * n_u
+    per_outer = 2 * (288.0 * nel + 16.0 * nnod + 8.0 * n_p) + (5 * n_p + 2 * n_u) * 8.0 + 4 * 16.0 * n_p
+    return inner * per_inner + outer * per_outer
 
 
 class _Null:

@@ -82,3 +82,20 @@ def test_tuning_record_replays(tmp_path):
     o2 = batch.tuned_opts(_Ctx(32, 256), loaded)
     assert o2 == batch.FAST
     assert batch.tuning_key(_Ctx(16, 128, 0)) == "16x128/continuous"
+
+
+def test_solve_bytes_model():
+    """The per-solve byte model is linear in the iteration counts, and its
+    V-cycle stops at the dense coarsest level (4x32 under coarse_max 1536)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    m = bench.solve_bytes_model
+    base = m(128, 1024, 0, 0)
+    assert base == 0.0
+    one_in, one_out = m(128, 1024, 0, 1), m(128, 1024, 1, 0)
+    assert m(128, 1024, 904, 2949) == pytest.approx(904 * one_out + 2949 * one_in)
+    # the fine-level FP32 applies alone: 6 per V-cycle of 90.2 MB
+    assert one_in > 6 * (312 * 262144 + 16 * 526336)
+    # the dense coarsest (1,152 DOFs) is part of every V-cycle, and a mesh that
+    # is its own coarsest level is the dense apply plus the Krylov work
+    assert m(4, 32, 0, 1) == pytest.approx(1152 ** 2 * 8 + 624 * 256 + 48 * 576 + 128 * 1152)
