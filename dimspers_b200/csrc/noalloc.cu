@@ -2,12 +2,17 @@
 //
 // dp_apply_K stages x and y in the lattice numbering through work vectors the
 // context allocated with cudaMalloc.  Some callers cannot allocate at all:
-// code running while a CUDA stream is being captured into a graph (cudaMalloc
-// is not allowed there), hosts whose device memory is owned by a pool or
-// allocator that the library must not bypass, and real-time loops that forbid
-// allocation after start-up.  dp_apply_K_noalloc does the same apply with its
-// two staging vectors in one static device array of this file instead, and
-// calls no cudaMalloc / cudaFree / allocating library routine.
+// hosts whose device memory is owned by a pool or allocator of their own that
+// the library must not bypass, and real-time loops that forbid allocation
+// after start-up (cudaMalloc / cudaFree may synchronise the device and take
+// unbounded time).  dp_apply_K_noalloc does the same apply with its two
+// staging vectors in one static device array of this file instead, and calls
+// no cudaMalloc / cudaFree / allocating library routine.
+//
+// Ordering: the call reads x and writes y on the context's stream and returns
+// after synchronising that stream.  It does not wait for other streams, so
+// the caller must have finished producing x (and consuming y) first, e.g. by
+// synchronising the stream that wrote x.
 //
 // Limits and sharing:
 //   - the array holds kNoAllocScratchDoubles doubles (32 MiB); a mesh needs

@@ -224,14 +224,19 @@ int dp_get_rhs(dp_ctx* ctx, double* F, double* pc);
 
 void dp_default_opts(dp_solve_opts* opts);
 
-/* y = K x like dp_apply_K, for callers that cannot allocate device memory
- * (inside a stream capture, under an external allocator, after start-up in a
- * real-time loop).  No counterpart in the reference.  x and y are DEVICE
- * pointers (2*nnod, reference numbering); the two staging vectors live in one
- * static 32 MiB device array of the library, so nnod <= 1,048,576 (larger
- * meshes: DP_BAD_ARG).  No cudaMalloc/cudaFree is called.  All calls on a
- * device share that array: calls that overlap on the GPU race.  The first call
- * on a device looks up the array's address; make it before any stream capture. */
+/* y = K x like dp_apply_K, for callers that cannot allocate device memory:
+ * hosts whose device memory is owned by their own pool or allocator, which the
+ * library must not bypass, and real-time loops that forbid allocation after
+ * start-up (cudaMalloc/cudaFree can synchronise the device and take unbounded
+ * time).  No counterpart in the reference.  x and y are DEVICE pointers
+ * (2*nnod, reference numbering); the two staging vectors live in one static
+ * 32 MiB device array of the library, so nnod <= 1,048,576 (larger meshes:
+ * DP_BAD_ARG).  No cudaMalloc/cudaFree is called.  The call runs on the
+ * context's stream and returns when that stream has finished it, so the
+ * caller must have finished writing x (and any reading of y) beforehand, e.g.
+ * by synchronising its own stream.  All calls on a device share that array:
+ * calls that overlap on the GPU race.  The first call on a device looks up the
+ * array's address; make it before any stream capture begins. */
 int dp_apply_K_noalloc(dp_ctx* ctx, const double* x, double* y);
 
 /* ---- strain-rate / stress post-processor --------------------------------

@@ -15,6 +15,7 @@ Restates:
   updatevelocity2        src/Stokes/StokesSolver.jl:170-184
   volume_integral        src/Stress/FSE.jl:412-464
 """
+import time
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -44,13 +45,16 @@ def lumped_pc(MM):
 
 
 def stokes_pcg(KK, MM, GG, Rhs, ifree, rtol=1e-8, itmax=200, itmin=10, permc="MMD_AT_PLUS_A",
-               schur_pc="lumped"):
+               schur_pc="lumped", timing=None):
     """StokesPcCG (IterativeSolvers.jl:94-168); returns U, P, report.
 
     schur_pc="lumped" is the reference's StokesPcCG (:jacobi -> 1/rowsum M);
     "mass" applies M^-1 with a direct factorisation of the symmetrised M, the
     `d = pc \\ r` of StokesPcCG_pardiso (:32-34, :82) whose incomplete LDL^T
-    (lldl) is exact for block-diagonal M (discontinuous pressure)."""
+    (lldl) is exact for block-diagonal M (discontinuous pressure).
+    timing: optional dict; receives "setup" (s, factorisation and first
+    solve) and "iters" (s per outer iteration, the whole loop body)."""
+    t_start = time.perf_counter()
     nU = Rhs.size
     U = np.zeros(nU)
     P = np.zeros(GG.shape[1])
@@ -71,6 +75,10 @@ def stokes_pcg(KK, MM, GG, Rhs, ifree, rtol=1e-8, itmax=200, itmin=10, permc="MM
     d = prec(r)
     q = d.copy()
     rep = PcgReport()
+    t_last = time.perf_counter()
+    if timing is not None:
+        timing["setup"] = t_last - t_start
+        timing["iters"] = []
     for it in range(1, itmax + 1):
         q = rm0space(q)
         rd = r @ d
@@ -88,10 +96,16 @@ def stokes_pcg(KK, MM, GG, Rhs, ifree, rtol=1e-8, itmax=200, itmin=10, permc="MM
         rep.history.append(nr)
         rep.iterations = it
         if nr < tol and it >= itmin:
+            if timing is not None:
+                timing["iters"].append(time.perf_counter() - t_last)
             break
         d = prec(r)
         beta = ((r - rlast) @ d) / rd
         q = d + beta * q
+        if timing is not None:
+            t = time.perf_counter()
+            timing["iters"].append(t - t_last)
+            t_last = t
     rep.relres = rep.history[-1] / (tol / rtol) if tol > 0 else 0.0
     return U, P, rep
 
@@ -157,11 +171,15 @@ def assemble(prob, eta_ip, rho_node, g, C6=None, elements=None):
 
 
 def solve_stokes(prob, eta_ip, rho_node, g, C6=None, rtol=1e-8, itmax=200, itmin=10,
-                 remove_rotation=True, schur_pc="lumped"):
-    """solveStokes (StokesSolver.jl:7-54), solver=:suitesparse."""
-    A = assemble(prob, eta_ip, rho_node, g, C6)
+                 remove_rotation=True, schur_pc="lumped", permc="MMD_AT_PLUS_A", elements=None, timing=None):
+    """solveStokes (StokesSolver.jl:7-54), solver=:suitesparse.
+    timing: optional dict, filled with "assembly" (s) and stokes_pcg's fields."""
+    t0 = time.perf_counter()
+    A = assemble(prob, eta_ip, rho_node, g, C6, elements=elements)
+    if timing is not None:
+        timing["assembly"] = time.perf_counter() - t0
     U, P, rep = stokes_pcg(A["KK"], A["MM"], A["GG"], A["F"], prob.ifree, rtol, itmax, itmin,
-                           schur_pc=schur_pc)
+                           permc=permc, schur_pc=schur_pc, timing=timing)
     Upol = U
     om = 0.0
     if remove_rotation:

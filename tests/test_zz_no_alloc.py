@@ -1,6 +1,6 @@
 """dp_apply_K_noalloc: the K-apply for callers that cannot allocate device
-memory (a stream being captured into a CUDA graph, an external allocator that
-owns the device memory, a real-time loop).  Its staging vectors live in a
+memory (a host whose own allocator owns the device memory, a real-time loop
+that forbids allocation after start-up).  Its staging vectors live in a
 static device array of the library instead of context work buffers; this
 file checks it against dp_apply_K through the C ABI on two calls in a row (the
 shared array keeps the previous call's contents), and that meshes beyond the
