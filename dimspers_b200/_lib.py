@@ -92,6 +92,7 @@ SIGNATURES = {
     "dp_apply_GT": (C.c_int, [_P, _P, _P, C.c_int32]),
     "dp_apply_K_noalloc": (C.c_int, [_P, _P, _P]),
     "dp_get_rhs": (C.c_int, [_P, _P, _P]),
+    "dp_reduce": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int32, _P, C.c_int32]),
     "dp_default_opts": (None, [C.POINTER(SolveOpts)]),
     "dp_profile_kernel": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     "dp_stress": (C.c_int, [_P, _P, _P, C.c_int64, C.POINTER(_P), C.c_int64, _P, C.c_int32]),

@@ -737,6 +737,35 @@ static int apply_common(dp_ctx* h, const double* in, double* out, int32_t mem, i
   });
 }
 
+int dp_reduce(dp_ctx* h, const double* a, const double* b, int64_t n, int32_t op, double* out, int32_t mem) {
+  if (!h) return DP_BAD_ARG;
+  Ctx& c = h->c;
+  return guarded(&c, [&] {
+    DP_CUDA(cudaSetDevice(c.device));
+    if (!a || !out || n < 0 || op < 0 || op > 3 || (op < 2 && !b)) throw BadArg("dp_reduce: bad argument");
+    const double* da = a;
+    const double* db = b;
+    double* tmp = nullptr;
+    if (mem == DP_MEM_HOST && n > 0) {
+      DP_CUDA(cudaMalloc(&tmp, sizeof(double) * 2 * n));
+      DP_CUDA(cudaMemcpyAsync(tmp, a, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
+      if (op < 2) DP_CUDA(cudaMemcpyAsync(tmp + n, b, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
+      da = tmp;
+      db = tmp + n;
+    }
+    const int slot = 40;
+    if (op == 0) launch_dot(c, da, db, n, slot);
+    else if (op == 1) launch_dot_c(c, da, db, n, slot);
+    else if (op == 2) launch_sum(c, da, n, slot);
+    else launch_sum_c(c, da, n, slot);
+    DP_CUDA(cudaMemcpyAsync(c.h_scal + slot, c.scal + slot, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    DP_CUDA(cudaStreamSynchronize(c.stream));
+    if (tmp) DP_CUDA(cudaFree(tmp));
+    *out = c.h_scal[slot];
+    return (int)DP_OK;
+  });
+}
+
 int dp_apply_K(dp_ctx* h, const double* x, double* y, int32_t mem) { return apply_common(h, x, y, mem, 0); }
 int dp_apply_G(dp_ctx* h, const double* p, double* y, int32_t mem) { return apply_common(h, p, y, mem, 1); }
 int dp_apply_GT(dp_ctx* h, const double* x, double* p, int32_t mem) { return apply_common(h, x, p, mem, 2); }

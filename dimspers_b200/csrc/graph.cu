@@ -452,9 +452,9 @@ static void emit_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
     emit_inner(c, cfg, c.F, Uz, 0, 0);
     launch_apply_GT(c, Uz, rz);
     klaunch(k_neg, g_nb(nP), 256, 0, c.stream, rz, nP);
-    launch_sum(c, rz, nP, S_SUMR);
+    launch_sum_c(c, rz, nP, S_SUMR);
     klaunch(k_sub_mean, g_nb(nP), 256, 0, c.stream, rz, nP, c.scal + S_SUMR);
-    launch_dot(c, rz, rz, nP, G_RZREF);
+    launch_dot_c(c, rz, rz, nP, G_RZREF);
   }
   // Rhs = F + G P ; U = K^-1 Rhs (tight inner tolerance) ; r = -G^T U ;
   // rm0space!(r) ; ||r||^2 -> S_RR.  The initial residual, and in the restart
@@ -465,9 +465,9 @@ static void emit_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
     emit_inner(c, cfg, rhs, U, depth, 0);
     launch_apply_GT(c, U, r);
     klaunch(k_neg, g_nb(nP), 256, 0, c.stream, r, nP);
-    launch_sum(c, r, nP, S_SUMR);
+    launch_sum_c(c, r, nP, S_SUMR);
     klaunch(k_sub_mean, g_nb(nP), 256, 0, c.stream, r, nP, c.scal + S_SUMR);
-    launch_dot(c, r, r, nP, S_RR);
+    launch_dot_c(c, r, r, nP, S_RR);
   };
   // d = r .* pc (or M^-1 r) ; q = d
   auto pc_start = [&] {
@@ -477,7 +477,7 @@ static void emit_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
       klaunch(k_mul_into, g_nb(nP), 256, 0, c.stream, r, c.pc, d, nP);
     }
     DP_CUDA(cudaMemcpyAsync(q, d, sizeof(double) * nP, cudaMemcpyDeviceToDevice, c.stream));
-    launch_sum(c, q, nP, S_SUMQ);
+    launch_sum_c(c, q, nP, S_SUMQ);
   };
   // the StokesPcCG iteration (IterativeSolvers.jl:130-166) as a WHILE body
   auto outer_body = [&](cudaGraphConditionalHandle h, int depth) {
@@ -485,7 +485,7 @@ static void emit_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
     launch_apply_G(c, q, y);
     emit_inner(c, cfg, y, z, depth + 1, cfg.inner_relax > 0.0 ? 1 : 0);
     launch_apply_GT(c, z, Sq);
-    launch_dot(c, q, Sq, nP, S_QSQ);
+    launch_dot_c(c, q, Sq, nP, S_QSQ);
     klaunch(k_schur_update_p, red_grid(nP), kRedThreads, 0, c.stream, P, r, rlast, q, Sq, nP, c.scal, c.partial,
             c.counter);
     klaunch(k_axpy_slot, g_nb(nU), 256, 0, c.stream, U, z, nU, c.scal);
@@ -540,9 +540,9 @@ static void emit_solve(Ctx& c, const SolveCfg& cfg, double* U, double* P) {
   launch_dot(c, rhs, rhs, nU, S_TMP);
   launch_dot(c, c.F, c.F, nU, S_TMP2);
   launch_apply_GT(c, U, Sq);
-  launch_sum(c, Sq, nP, S_SUMR);
+  launch_sum_c(c, Sq, nP, S_SUMR);
   klaunch(k_sub_mean, g_nb(nP), 256, 0, c.stream, Sq, nP, c.scal + S_SUMR);
-  launch_dot(c, Sq, Sq, nP, G_TMP3);
+  launch_dot_c(c, Sq, Sq, nP, G_TMP3);
   if (cfg.remove_rotation) {
     klaunch(k_rot_integrals, red_grid(L.nel), kRedThreads, 0, c.stream, U, c.rho_lat, c.theta_lat, c.r_lat, (int)L.nel, L.ncr,
                                                                    (int)L.A(), (int)L.B(), c.scal, c.partial, c.counter);

@@ -31,6 +31,9 @@ void launch_apply_GT(Ctx& c, const double* x, double* p);    // p = G^T x (zeroe
 void launch_dot(Ctx& c, const double* a, const double* b, int64_t n, int slot);
 void launch_dot_f(Ctx& c, const float* a, const float* b, int64_t n, int slot);
 void launch_sum(Ctx& c, const double* a, int64_t n, int slot);
+// compensated (double-double) dot and sum: the Schur-complement reductions
+void launch_dot_c(Ctx& c, const double* a, const double* b, int64_t n, int slot);
+void launch_sum_c(Ctx& c, const double* a, int64_t n, int slot);
 void launch_gather_ref2lat(Ctx& c, const double* ref, double* lat, int comps);
 void launch_scatter_lat2ref(Ctx& c, const double* lat, double* ref, int comps);
 void launch_pc_invert(Ctx& c, double* pc, int64_t n);

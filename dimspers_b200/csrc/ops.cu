@@ -370,7 +370,39 @@ __global__ void __launch_bounds__(kRedThreads) k_sum(const double* __restrict__ 
   grid_finish<1>(v, partial, counter, o);
 }
 
+// compensated variants (double-double accumulation) for the Schur-complement loop
+__global__ void __launch_bounds__(kRedThreads) k_dot_c(const double* __restrict__ a, const double* __restrict__ b,
+                                                       int64_t n, double* partial, unsigned int* counter, double* out) {
+  grid_dep_wait();
+  DD s{0.0, 0.0};
+  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads)
+    dd_add_prod(s, a[i], b[i]);
+  DD v[1] = {s};
+  double* o[1] = {out};
+  grid_finish_dd<1>(v, partial, counter, o);
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_sum_c(const double* __restrict__ a, int64_t n, double* partial,
+                                                       unsigned int* counter, double* out) {
+  grid_dep_wait();
+  DD s{0.0, 0.0};
+  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads)
+    dd_add(s, a[i]);
+  DD v[1] = {s};
+  double* o[1] = {out};
+  grid_finish_dd<1>(v, partial, counter, o);
+}
+
 static int red_blocks(int64_t n) { return red_grid(n); }
+
+void launch_dot_c(Ctx& c, const double* a, const double* b, int64_t n, int slot) {
+  klaunch(k_dot_c, red_blocks(n), kRedThreads, 0, c.stream, a, b, n, c.partial, c.counter, c.scal + slot);
+  DP_LAUNCH_CHECK();
+}
+void launch_sum_c(Ctx& c, const double* a, int64_t n, int slot) {
+  klaunch(k_sum_c, red_blocks(n), kRedThreads, 0, c.stream, a, n, c.partial, c.counter, c.scal + slot);
+  DP_LAUNCH_CHECK();
+}
 
 void launch_dot(Ctx& c, const double* a, const double* b, int64_t n, int slot) {
   klaunch(k_dot<double>, red_blocks(n), kRedThreads, 0, c.stream, a, b, n, c.partial, c.counter, c.scal + slot);

@@ -54,18 +54,18 @@ __global__ void __launch_bounds__(kRedThreads) k_schur_update_p(double* __restri
                                                                  double* scal, double* partial, unsigned int* counter) {
   grid_dep_wait();
   const double alpha = scal[S_RD] / scal[S_QSQ];
-  double s = 0.0;
+  DD s{0.0, 0.0};
   for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
     const double ri = r[i];
     rlast[i] = ri;
     P[i] += alpha * q[i];
     const double rn = ri - alpha * Sq[i];
     r[i] = rn;
-    s += rn;
+    dd_add(s, rn);
   }
-  double v[1] = {s};
+  DD v[1] = {s};
   double* o[1] = {scal + S_SUMR};
-  grid_finish<1>(v, partial, counter, o);
+  grid_finish_dd<1>(v, partial, counter, o);
 }
 
 __global__ void k_axpy_slot(double* __restrict__ U, const double* __restrict__ z, int64_t n, const double* scal) {
@@ -82,18 +82,18 @@ __global__ void __launch_bounds__(kRedThreads) k_schur_center(double* __restrict
                                                                unsigned int* counter) {
   grid_dep_wait();
   const double m = scal[S_SUMR] / (double)n;
-  double s0 = 0.0, s1 = 0.0;
+  DD s0{0.0, 0.0}, s1{0.0, 0.0};
   for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
     const double ri = r[i] - m;
     r[i] = ri;
     const double di = ri * pc[i];
     d[i] = di;
-    s0 += ri * ri;
-    s1 += (ri - rlast[i]) * di;
+    dd_add_prod(s0, ri, ri);
+    dd_add_prod(s1, ri - rlast[i], di);
   }
-  double v[2] = {s0, s1};
+  DD v[2] = {s0, s1};
   double* o[2] = {scal + S_RR, scal + S_BNUM};
-  grid_finish<2>(v, partial, counter, o);
+  grid_finish_dd<2>(v, partial, counter, o);
 }
 
 // Element-block mass preconditioner (discontinuous pressure): d_e = M_e^-1 r_e.
@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(kRedThreads) k_schur_center_blk(double* __rest
                                                                    unsigned int* counter) {
   grid_dep_wait();
   const double m = scal[S_SUMR] / (3.0 * (double)nel);
-  double s0 = 0.0, s1 = 0.0;
+  DD s0{0.0, 0.0}, s1{0.0, 0.0};
   for (int e = blockIdx.x * kRedThreads + threadIdx.x; e < nel; e += gridDim.x * kRedThreads) {
     double rv[3];
     for (int k = 0; k < 3; ++k) {
@@ -130,13 +130,13 @@ __global__ void __launch_bounds__(kRedThreads) k_schur_center_blk(double* __rest
                           c * rv[0] + f * rv[1] + g * rv[2]};
     for (int k = 0; k < 3; ++k) {
       d[3 * (size_t)e + k] = dv[k];
-      s0 += rv[k] * rv[k];
-      s1 += (rv[k] - rlast[3 * (size_t)e + k]) * dv[k];
+      dd_add_prod(s0, rv[k], rv[k]);
+      dd_add_prod(s1, rv[k] - rlast[3 * (size_t)e + k], dv[k]);
     }
   }
-  double v[2] = {s0, s1};
+  DD v[2] = {s0, s1};
   double* o[2] = {scal + S_RR, scal + S_BNUM};
-  grid_finish<2>(v, partial, counter, o);
+  grid_finish_dd<2>(v, partial, counter, o);
 }
 
 // q = d + beta q, beta = BNUM / RD; sum(q) -> S_SUMQ (for the next rm0space!)
@@ -144,15 +144,15 @@ __global__ void __launch_bounds__(kRedThreads) k_q_update(double* __restrict__ q
                                                            double* scal, double* partial, unsigned int* counter) {
   grid_dep_wait();
   const double beta = scal[S_BNUM] / scal[S_RD];
-  double s = 0.0;
+  DD s{0.0, 0.0};
   for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
     const double qi = d[i] + beta * q[i];
     q[i] = qi;
-    s += qi;
+    dd_add(s, qi);
   }
-  double v[1] = {s};
+  DD v[1] = {s};
   double* o[1] = {scal + S_SUMQ};
-  grid_finish<1>(v, partial, counter, o);
+  grid_finish_dd<1>(v, partial, counter, o);
 }
 
 // q -= mean(q); rd = r.d -> S_RD
@@ -161,14 +161,14 @@ __global__ void __launch_bounds__(kRedThreads) k_q_center_rd(double* __restrict_
                                                               double* partial, unsigned int* counter) {
   grid_dep_wait();
   const double m = scal[S_SUMQ] / (double)n;
-  double s = 0.0;
+  DD s{0.0, 0.0};
   for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
     q[i] -= m;
-    s += r[i] * d[i];
+    dd_add_prod(s, r[i], d[i]);
   }
-  double v[1] = {s};
+  DD v[1] = {s};
   double* o[1] = {scal + S_RD};
-  grid_finish<1>(v, partial, counter, o);
+  grid_finish_dd<1>(v, partial, counter, o);
 }
 
 __global__ void k_mul_into(const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out,
@@ -389,7 +389,7 @@ __global__ void __launch_bounds__(kRedThreads) k_rot_integrals(const double* __r
                                                                 int B, double* scal, double* partial,
                                                                 unsigned int* counter) {
   grid_dep_wait();
-  double am = 0.0, mom = 0.0;
+  DD am{0.0, 0.0}, mom{0.0, 0.0};
   for (int e = blockIdx.x * kRedThreads + threadIdx.x; e < nel; e += gridDim.x * kRedThreads) {
     int nd[6];
     element_nodes_mg(e, ncr, A, B, nd);
@@ -410,13 +410,13 @@ __global__ void __launch_bounds__(kRedThreads) k_rot_integrals(const double* __r
       const double om = r_ip * detJ * c_w[ip];
       double sa = 0.0, sm = 0.0;
       for (int k = 0; k < 6; ++k) { sa += va[k] * c_N[ip][k]; sm += vm[k] * c_N[ip][k]; }
-      am += sa * om;
-      mom += sm * om;
+      dd_add_prod(am, sa, om);
+      dd_add_prod(mom, sm, om);
     }
   }
-  double v[2] = {am, mom};
+  DD v[2] = {am, mom};
   double* o[2] = {scal + S_AM, scal + S_MOM};
-  grid_finish<2>(v, partial, counter, o);
+  grid_finish_dd<2>(v, partial, counter, o);
 }
 
 __global__ void k_rot_remove(double* __restrict__ U, const double* __restrict__ r_lat, int64_t nnod, const double* scal) {
@@ -463,9 +463,9 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
   // r = -G^T U; rm0space!(r)
   launch_apply_GT(c, U, r);
   klaunch(k_neg, nb256(nP), 256, 0, c.stream, r, nP);
-  launch_sum(c, r, nP, S_SUMR);
+  launch_sum_c(c, r, nP, S_SUMR);
   klaunch(k_sub_mean, nb256(nP), 256, 0, c.stream, r, nP, c.scal + S_SUMR);
-  launch_dot(c, r, r, nP, S_RR);
+  launch_dot_c(c, r, r, nP, S_RR);
   DP_LAUNCH_CHECK();
   const double r0 = std::sqrt(read_slot(c, S_RR));
   res.r0 = r0;
@@ -477,7 +477,7 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
     klaunch(k_mul_into, nb256(nP), 256, 0, c.stream, r, c.pc, d, nP);
   }
   DP_CUDA(cudaMemcpyAsync(q, d, sizeof(double) * nP, cudaMemcpyDeviceToDevice, c.stream));
-  launch_sum(c, q, nP, S_SUMQ);
+  launch_sum_c(c, q, nP, S_SUMQ);
   res.status = 1;  // not converged until shown otherwise
   res.iterations = 0;
   double rnorm = r0;
@@ -489,7 +489,7 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
     launch_apply_G(c, q, y);
     inner_solve(c, y, z, cfg, st);
     launch_apply_GT(c, z, Sq);
-    launch_dot(c, q, Sq, nP, S_QSQ);
+    launch_dot_c(c, q, Sq, nP, S_QSQ);
     // P += alpha q; U += alpha z; r -= alpha Sq
     klaunch(k_schur_update_p, red_grid(nP), kRedThreads, 0, c.stream, P, r, rlast, q, Sq, nP, c.scal, c.partial, c.counter);
     klaunch(k_axpy_slot, nb256(nU), 256, 0, c.stream, U, z, nU, c.scal);
@@ -533,9 +533,9 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
   read_slots(c, S_TMP, 2);
   res.mom_residual = std::sqrt(c.h_scal[S_TMP] / std::max(c.h_scal[S_TMP2], 1e-300));
   launch_apply_GT(c, U, Sq);
-  launch_sum(c, Sq, nP, S_SUMR);
+  launch_sum_c(c, Sq, nP, S_SUMR);
   klaunch(k_sub_mean, nb256(nP), 256, 0, c.stream, Sq, nP, c.scal + S_SUMR);
-  launch_dot(c, Sq, Sq, nP, S_TMP);
+  launch_dot_c(c, Sq, Sq, nP, S_TMP);
   res.div_residual = r0 > 0.0 ? std::sqrt(read_slot(c, S_TMP)) / r0 : 0.0;
 
   // rigid-rotation removal (updatevelocity2)

@@ -200,6 +200,19 @@ class StokesContext:
         self._chk(lib().dp_apply_K(self.h, _ptr(x), _ptr(y), DP_MEM_HOST))
         return y
 
+    def reduce(self, a, b=None, compensated=True):
+        """The solver's deterministic reduction of host vectors: sum a_i b_i
+        (b given) or sum a_i, compensated (the Schur loop's) or plain."""
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        op = (0 if b is not None else 2) + (1 if compensated else 0)
+        bp = None
+        if b is not None:
+            b = np.ascontiguousarray(b, dtype=np.float64)
+            bp = _ptr(b)
+        out = C.c_double(0.0)
+        self._chk(lib().dp_reduce(self.h, _ptr(a), bp, a.size, op, C.byref(out), DP_MEM_HOST))
+        return out.value
+
     def apply_G(self, p):
         p = np.ascontiguousarray(p, dtype=np.float64)
         y = np.empty(2 * self.nnod)

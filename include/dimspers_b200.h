@@ -218,6 +218,13 @@ int dp_solve(dp_ctx* ctx, double* U, double* P, double* Ucart, const dp_solve_op
 int dp_apply_K(dp_ctx* ctx, const double* x, double* y, int32_t mem);
 int dp_apply_G(dp_ctx* ctx, const double* p, double* y, int32_t mem);
 int dp_apply_GT(dp_ctx* ctx, const double* x, double* p, int32_t mem);
+/* The deterministic reductions of the solver, on caller vectors of length n
+ * (host or device per mem): op 0 = sum a_i b_i, 1 = the same compensated
+ * (double-double accumulation, the Schur-complement loop's dots), 2 = sum a_i,
+ * 3 = the same compensated (the loop's means).  Replaces mydot/mynorm and the
+ * sums of vmean (src/Algebra/Algebra.jl:104-113, src/IterativeSolvers.jl:
+ * 172-186), which the reference computes in plain FP64. */
+int dp_reduce(dp_ctx* ctx, const double* a, const double* b, int64_t n, int32_t op, double* out, int32_t mem);
 /* Assembled right-hand side (polar, reference numbering) and lumped pressure
  * preconditioner 1/rowsum(M). */
 int dp_get_rhs(dp_ctx* ctx, double* F, double* pc);

@@ -12,7 +12,7 @@ StokesPcCG) run far below the 1e-8 stopping tolerance.  This script makes:
             noise floor (the same solve with a second column ordering of the LU)
             -> config1_32x256_iso_disc.npz + tight.json["config1"]
   tight128  128x1024 anisotropic workload (contrast 1e5, seed 1, discontinuous
-            P1): U and P at rtol 1e-10 with the exact element-mass Schur
+            P1): U and P at rtol 1e-12 with the exact element-mass Schur
             preconditioner; every 15th entry is kept (odd stride: both velocity
             components) with the full norms -> tight_128x1024_aniso.npz
   refsolve  completed oracle solves of the reference algorithm (lumped Schur
@@ -115,13 +115,13 @@ def tight128():
     mat = inputs.make_material(MeshView(prob), "aniso", seed=1)
     tm = {}
     t0 = time.perf_counter()
-    s = OS.solve_stokes(prob, mat.eta_ip, mat.rho, mat.g, mat.C6, rtol=1e-10, itmax=20000, schur_pc="mass",
+    s = OS.solve_stokes(prob, mat.eta_ip, mat.rho, mat.g, mat.C6, rtol=1e-12, itmax=20000, schur_pc="mass",
                         elements=elements(), timing=tm)
     U, P = s["U"], s["P"]
     np.savez_compressed(os.path.join(HERE, "tight_128x1024_aniso.npz"), U_sub=U[::STRIDE], P_sub=P[::STRIDE],
                         U_norm=np.linalg.norm(U), P_norm=np.linalg.norm(P), stride=STRIDE)
     merge("tight128", dict(nr_cells=128, ntheta_cells=1024, pressure="discontinuous", kind="aniso", seed=1,
-                           schur_pc="mass", rtol=1e-10, iterations=s["report"].iterations,
+                           schur_pc="mass", rtol=1e-12, iterations=s["report"].iterations,
                            relres=s["report"].relres, seconds=time.perf_counter() - t0, stride=STRIDE))
     print("tight128", s["report"].iterations, flush=True)
 
