@@ -111,6 +111,7 @@ SIGNATURES = {
                                 C.POINTER(_P)]),
     "dp_cnn_destroy": (None, [_P]),
     "dp_cnn_num_params": (C.c_int64, [_P]),
+    "dp_cnn_set_math": (C.c_int, [_P, C.c_int32]),
     "dp_cnn_set_params": (C.c_int, [_P, _P, C.c_int64]),
     "dp_cnn_get_params": (C.c_int, [_P, _P, _P, C.c_int64]),
     "dp_cnn_forward": (C.c_int, [_P, _P, _P, C.c_int32]),

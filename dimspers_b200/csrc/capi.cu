@@ -803,7 +803,7 @@ int dp_profile_kernel(dp_ctx* h, int32_t which, int32_t reps, int32_t flush_l2, 
     if (which == 5 && c.fabric_dem[0] == 0)
       throw BadArg("no staged DEM tensor inputs (call dp_anisotropic_tensor first)");
     if (which == 6 && !c.th_buf) throw BadArg("no thermal element blocks (call dp_thermal_step first)");
-    if (which < 0 || which > 6) throw BadArg("which must be 0..6");
+    if (which < 0 || which > 7) throw BadArg("which must be 0..7");
     const int64_t n = 2 * c.fine.nnod;
     double* x64 = (double*)c.work[W_IN_P];
     double* y64 = (double*)c.work[W_IN_AP];
@@ -822,6 +822,7 @@ int dp_profile_kernel(dp_ctx* h, int32_t which, int32_t reps, int32_t flush_l2, 
       else if (which == 4) launch_viscosity_staged(c);
       else if (which == 5) launch_dem_staged(c);
       else if (which == 6) launch_th_apply_staged(c);
+      else if (which == 7) profile_inner_vector_kernels(c);
       else if (c.mg_prec == 1) mg_apply_f(c, x32, y32, MGOptions());
       else mg_apply(c, x64, y64, MGOptions());
     };

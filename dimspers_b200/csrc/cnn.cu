@@ -18,6 +18,8 @@
 // (discontinuous: the element's vertex values; continuous: vertex values) and
 // handed to dp_solve with use_guess = 2, which keeps it only if it lowers the
 // initial Schur residual.
+#include <cuda_bf16.h>
+
 #include <cmath>
 #include <vector>
 
@@ -28,6 +30,8 @@ constexpr int kCnnMaxLayers = 12;
 
 struct Cnn {
   int nrg = 0, ntg = 0, C = 16, L = 6, cin = 4, device = 0;
+  int bf16 = 1;                 // 1: BF16 tensor-core convolutions (FP32 accumulate), 0: FP32 CUDA cores
+  __nv_bfloat16* wk = nullptr;  // the BF16 B operand of the current tensor-core convolution
   int dil[kCnnMaxLayers];
   int bmax = 0;
   cudaStream_t stream = nullptr;
@@ -52,7 +56,7 @@ struct Cnn {
   ~Cnn() {
     cudaFree(param); cudaFree(grad); cudaFree(adam_m); cudaFree(adam_v);
     for (size_t i = 1; i < act.size(); ++i) cudaFree(act[i]);
-    cudaFree(dbuf0); cudaFree(dbuf1); cudaFree(partial); cudaFree(counter); cudaFree(loss);
+    cudaFree(dbuf0); cudaFree(dbuf1); cudaFree(partial); cudaFree(counter); cudaFree(loss); cudaFree(wk);
     cudaFreeHost(h_loss);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -96,6 +100,128 @@ __global__ void __launch_bounds__(256) k_conv_fwd(const float* __restrict__ X, c
     float v = acc[co];
     if (relu && v < 0.f) v = 0.f;
     Y[((int64_t)b * COUT + co) * plane + (int64_t)i * ntg + j] = v;
+  }
+}
+
+// ---- BF16 tensor-core convolutions (mma.sync m16n8k16, FP32 accumulation) ----------
+// The forward convolution and the data gradient are both implicit GEMMs over
+// the grid points: out[p][n] = sum_tap sum_k in[k][p + s*tap] * B[tap][n][k],
+// with s = +1 (forward: k = input channel, n = output channel) or s = -1 (data
+// gradient: k = output channel, n = input channel).  One warp computes 16
+// consecutive theta points of one row times all NT*8 output columns; the K
+// loop runs over the 9 taps and blocks of 16 channels.  A fragments are
+// gathered from the FP32 activations and rounded to BF16; the B operand is
+// the layer's weights rounded to BF16, laid out [tap][n][k] with a row stride
+// of kpad + 8 elements, so the k pairs read from shared memory by a warp fall
+// in distinct banks.
+constexpr int kTcWarps = 4;
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);   // .x (low half) = lo
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// D += A B for one 16x8x16 tile: A rows = grid points, columns = k; B = k x n.
+// Fragment layout (PTX ISA, mma.m16n8k16 with .bf16): a[0] = (row g, k 2t..2t+1),
+// a[1] = (row g+8, k 2t..2t+1), a[2] = (row g, k 2t+8..2t+9), a[3] = (row g+8,
+// k 2t+8..2t+9); b0 = (k 2t..2t+1, col g), b1 = (k 2t+8..2t+9, col g); d[0..1] =
+// (row g, col 2t..2t+1), d[2..3] = (row g+8, col 2t..2t+1), with g = lane/4,
+// t = lane%4.
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// B operand of one layer: Bk[tap][n][k] (row stride kpad + 8) from W[co][ci][tap];
+// forward n = co, k = ci; data gradient n = ci, k = co.  Zero outside the layer.
+__global__ void k_conv_weights_bf16(const float* __restrict__ W, __nv_bfloat16* __restrict__ Bk, int cin, int cout,
+                                    int npad, int kpad, int transpose) {
+  const int ks = kpad + 8;
+  const int total = 9 * npad * ks;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    const int tap = idx / (npad * ks), rem = idx % (npad * ks), n = rem / ks, k = rem % ks;
+    const int co = transpose ? k : n, ci = transpose ? n : k;
+    float v = 0.f;
+    if (k < kpad && co < cout && ci < cin) v = W[(co * cin + ci) * 9 + tap];
+    Bk[idx] = __float2bfloat16_rn(v);
+  }
+}
+
+// out[b][n][i][j] = bias[n] + sum_tap sum_k X[b][k][i + s(ti-1)d][j + s(tj-1)d] Bk[tap][n][k]
+// (zero rows outside [0, nrg), periodic in j), ReLU optional.  ntg % 16 == 0.
+template <int NT>
+__global__ void __launch_bounds__(kTcWarps * 32) k_conv_tc(const float* __restrict__ X,
+                                                           const __nv_bfloat16* __restrict__ Bk,
+                                                           const float* __restrict__ bias, float* __restrict__ Y,
+                                                           int kch, int kpad, int nch, int nrg, int ntg, int dil,
+                                                           int sgn, int relu) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __nv_bfloat16* sb = reinterpret_cast<__nv_bfloat16*>(smem_raw);
+  const int ks = kpad + 8;
+  const int nb_words = (9 * NT * 8 * ks) / 2;
+  const uint32_t* gsrc = reinterpret_cast<const uint32_t*>(Bk);
+  uint32_t* sdst = reinterpret_cast<uint32_t*>(sb);
+  for (int w = threadIdx.x; w < nb_words; w += blockDim.x) sdst[w] = gsrc[w];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int b = blockIdx.z, i = blockIdx.y;
+  const int j0 = (blockIdx.x * kTcWarps + warp) * 16;
+  if (j0 >= ntg) return;                      // whole warps only (ntg is a multiple of 16)
+  const int64_t plane = (int64_t)nrg * ntg;
+  const float* Xb = X + (int64_t)b * kch * plane;
+  float acc[NT][4];
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[nt][q] = 0.f;
+  for (int ti = 0; ti < 3; ++ti) {
+    const int ii = i + sgn * (ti - 1) * dil;
+    if (ii < 0 || ii >= nrg) continue;        // the same for the whole warp
+    const float* row = Xb + (int64_t)ii * ntg;
+    for (int tj = 0; tj < 3; ++tj) {
+      int ja = j0 + g + sgn * (tj - 1) * dil;
+      int jb = ja + 8;
+      ja = ((ja % ntg) + ntg) % ntg;
+      jb = ((jb % ntg) + ntg) % ntg;
+      const __nv_bfloat16* bt = sb + (ti * 3 + tj) * NT * 8 * ks;
+      for (int k0 = 0; k0 < kpad; k0 += 16) {
+        const int c0 = k0 + 2 * t, c1 = c0 + 1, c2 = c0 + 8, c3 = c0 + 9;
+        const float x0a = c0 < kch ? row[(int64_t)c0 * plane + ja] : 0.f;
+        const float x1a = c1 < kch ? row[(int64_t)c1 * plane + ja] : 0.f;
+        const float x0b = c0 < kch ? row[(int64_t)c0 * plane + jb] : 0.f;
+        const float x1b = c1 < kch ? row[(int64_t)c1 * plane + jb] : 0.f;
+        const float x2a = c2 < kch ? row[(int64_t)c2 * plane + ja] : 0.f;
+        const float x3a = c3 < kch ? row[(int64_t)c3 * plane + ja] : 0.f;
+        const float x2b = c2 < kch ? row[(int64_t)c2 * plane + jb] : 0.f;
+        const float x3b = c3 < kch ? row[(int64_t)c3 * plane + jb] : 0.f;
+        const uint32_t a[4] = {pack_bf16(x0a, x1a), pack_bf16(x0b, x1b), pack_bf16(x2a, x3a), pack_bf16(x2b, x3b)};
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+          const __nv_bfloat16* bn = bt + (nt * 8 + g) * ks + k0 + 2 * t;
+          const uint32_t b0 = *reinterpret_cast<const uint32_t*>(bn);
+          const uint32_t b1 = *reinterpret_cast<const uint32_t*>(bn + 8);
+          mma_bf16_16816(acc[nt], a, b0, b1);
+        }
+      }
+    }
+  }
+  float* Yb = Y + (int64_t)b * nch * plane + (int64_t)i * ntg;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int n = nt * 8 + 2 * t + (q & 1);
+      const int j = j0 + g + ((q & 2) ? 8 : 0);
+      if (n < nch) {
+        float v = acc[nt][q] + (bias ? bias[n] : 0.f);
+        if (relu && v < 0.f) v = 0.f;
+        Yb[(int64_t)n * plane + j] = v;
+      }
+    }
   }
 }
 
@@ -255,9 +381,59 @@ static void conv_bwd_data(Cnn& n, int l, const float* dY, float* dX, int nb) {
   DP_LAUNCH_CHECK();
 }
 
+// ---- tensor-core dispatch ------------------------------------------------------------
+static int pad16(int c) { return (c + 15) / 16 * 16; }
+static int ntiles(int c) { return (c + 7) / 8; }
+// elements of a layer's B operand: forward (n = cout, k = cin) or data gradient (n = cin, k = cout)
+static int64_t wk_elems(int cin, int cout, bool transpose) {
+  const int nch = transpose ? cin : cout, kch = transpose ? cout : cin;
+  return 9LL * ntiles(nch) * 8 * (pad16(kch) + 8);
+}
+static bool tc_ok(const Cnn& n) { return n.bf16 && n.ntg % 16 == 0; }
+
+template <int NT>
+static void conv_tc_n(Cnn& n, const float* X, const __nv_bfloat16* Bk, const float* bias, float* Y, int kch, int nch,
+                      int dil, int sgn, int relu, int nb) {
+  const int kpad = pad16(kch);
+  const size_t smem = sizeof(__nv_bfloat16) * 9 * NT * 8 * (kpad + 8);
+  dim3 grid((unsigned)div_up(n.ntg, 16 * kTcWarps), (unsigned)n.nrg, (unsigned)nb);
+  ++g_klaunch;
+  k_conv_tc<NT><<<grid, kTcWarps * 32, smem, n.stream>>>(X, Bk, bias, Y, kch, kpad, nch, n.nrg, n.ntg, dil, sgn,
+                                                          relu);
+  DP_LAUNCH_CHECK();
+}
+static void conv_tc(Cnn& n, const float* X, const __nv_bfloat16* Bk, const float* bias, float* Y, int kch, int nch,
+                    int dil, int sgn, int relu, int nb) {
+  switch (ntiles(nch)) {
+    case 1: conv_tc_n<1>(n, X, Bk, bias, Y, kch, nch, dil, sgn, relu, nb); break;
+    case 2: conv_tc_n<2>(n, X, Bk, bias, Y, kch, nch, dil, sgn, relu, nb); break;
+    case 4: conv_tc_n<4>(n, X, Bk, bias, Y, kch, nch, dil, sgn, relu, nb); break;
+    default: throw std::runtime_error("unsupported channel count");
+  }
+}
+// rounds layer l's weights to the BF16 B operand (forward or data gradient) in n.wk
+static const __nv_bfloat16* conv_weights(Cnn& n, int l, bool transpose) {
+  const int cin = n.cin_of(l), cout = n.cout_of(l);
+  const int nch = transpose ? cin : cout, kch = transpose ? cout : cin;
+  const int64_t total = wk_elems(cin, cout, transpose);
+  ++g_klaunch;
+  k_conv_weights_bf16<<<(int)std::min<int64_t>(div_up(total, 256), 1024), 256, 0, n.stream>>>(
+      n.param + n.woff[l], n.wk, cin, cout, ntiles(nch) * 8, pad16(kch), transpose ? 1 : 0);
+  DP_LAUNCH_CHECK();
+  return n.wk;
+}
+
 static void cnn_forward(Cnn& n, const float* x, int nb) {
   n.act[0] = const_cast<float*>(x);
-  for (int l = 0; l < n.L; ++l) conv_fwd(n, l, n.act[l], n.act[l + 1], nb);
+  for (int l = 0; l < n.L; ++l) {
+    if (tc_ok(n)) {
+      const __nv_bfloat16* Bk = conv_weights(n, l, false);
+      conv_tc(n, n.act[l], Bk, n.param + n.boff[l], n.act[l + 1], n.cin_of(l), n.cout_of(l), n.dil[l], 1,
+              l < n.L - 1 ? 1 : 0, nb);
+    } else {
+      conv_fwd(n, l, n.act[l], n.act[l + 1], nb);
+    }
+  }
 }
 
 // forward + backward; returns the device loss in n.loss
@@ -281,7 +457,12 @@ static void cnn_fwd_bwd(Cnn& n, const float* x, const float* t, int nb) {
                                                    n.nrg, n.ntg, n.dil[l]);
     DP_LAUNCH_CHECK();
     if (l > 0) {
-      conv_bwd_data(n, l, g, g2, nb);
+      if (tc_ok(n)) {
+        const __nv_bfloat16* Bk = conv_weights(n, l, true);
+        conv_tc(n, g, Bk, nullptr, g2, cout, cin, n.dil[l], -1, 0, nb);
+      } else {
+        conv_bwd_data(n, l, g, g2, nb);
+      }
       std::swap(g, g2);
     }
   }
@@ -388,6 +569,10 @@ int dp_cnn_create(int32_t nrg, int32_t ntg, int32_t channels, int32_t layers, co
     const int64_t gmax = (int64_t)max_batch * std::max(channels, 4) * plane;
     DP_CUDA(cudaMalloc(&n.dbuf0, sizeof(float) * gmax));
     DP_CUDA(cudaMalloc(&n.dbuf1, sizeof(float) * gmax));
+    int64_t wmax = 0;
+    for (int l = 0; l < layers; ++l)
+      wmax = std::max({wmax, wk_elems(n.cin_of(l), n.cout_of(l), false), wk_elems(n.cin_of(l), n.cout_of(l), true)});
+    DP_CUDA(cudaMalloc(&n.wk, sizeof(__nv_bfloat16) * wmax));
     DP_CUDA(cudaMalloc(&n.partial, sizeof(double) * 4 * kRedBlocks));
     DP_CUDA(cudaMalloc(&n.counter, sizeof(unsigned int)));
     DP_CUDA(cudaMemset(n.counter, 0, sizeof(unsigned int)));
@@ -411,6 +596,12 @@ void dp_cnn_destroy(dp_cnn* h) {
 }
 
 int64_t dp_cnn_num_params(const dp_cnn* h) { return h ? h->n.nparam : -1; }
+
+int dp_cnn_set_math(dp_cnn* h, int32_t bf16) {
+  if (!h || bf16 < 0 || bf16 > 1) return DP_BAD_ARG;
+  h->n.bf16 = bf16;
+  return DP_OK;
+}
 
 int dp_cnn_set_params(dp_cnn* h, const float* p, int64_t n) {
   if (!h || !p || n != h->n.nparam) return DP_BAD_ARG;

@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_upd_check(T* __restrict__ x
   }
   double v[1] = {s};
   double* o[1] = {scal + irr};
-  if (grid_finish<1>(v, partial, counter, o) && threadIdx.x == 0) {
+  if (grid_finish<1>(v, partial, counter, o) && threadIdx.x == 0 && ctl != nullptr) {
     int it;
     double tol2;
     if (fp32) { it = ++ctl->in32_it; tol2 = ctl->in32_tol2; ctl->in32_total += 1; }
@@ -576,6 +576,41 @@ static void ensure_ctl(Ctx& c) {
     DP_CUDA(cudaMallocHost(&c.h_ctl, sizeof(DevCtl)));
     for (int i = 0; i < 4; ++i) DP_CUDA(cudaStreamCreateWithFlags(&c.aux[i], cudaStreamNonBlocking));
   }
+}
+
+// The graph-only vector kernels of one inner iteration (FP64 Krylov, FP32
+// multigrid) launched once each outside a graph, without loop control: the
+// scaled FP32 residual, z = ||r|| z32 with r.z, the direction update and the
+// fused x/r update with ||r||^2.  Profilers cannot look inside conditional
+// graph nodes; this is what they time instead.  Vector contents are zeroed
+// and the scalars set to 1, so every value stays finite.
+void profile_inner_vector_kernels(Ctx& c) {
+  ensure_ctl(c);
+  const int64_t n = 2 * c.fine.nnod;
+  double* x = (double*)c.work[W_Z];
+  double* r = (double*)c.work[W_IN_R];
+  double* z = (double*)c.work[W_IN_Z];
+  double* p = (double*)c.work[W_IN_P];
+  double* Ap = (double*)c.work[W_IN_AP];
+  float* r32 = (float*)c.work[W_F_R];
+  float* z32 = (float*)c.work[W_F_Z];
+  DevCtl* ctl = (DevCtl*)c.ctl;
+  for (double* v : {x, r, z, p, Ap}) DP_CUDA(cudaMemsetAsync(v, 0, sizeof(double) * n, c.stream));
+  DP_CUDA(cudaMemsetAsync(r32, 0, sizeof(float) * n, c.stream));
+  DP_CUDA(cudaMemsetAsync(z32, 0, sizeof(float) * n, c.stream));
+  DP_CUDA(cudaMemsetAsync(&ctl->in_it, 0, sizeof(int), c.stream));
+  for (int k = 0; k < 4; ++k) c.h_scal[48 + k] = 1.0;
+  DP_CUDA(cudaMemcpyAsync(c.scal + G_RZ, c.h_scal + 48, 4 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+  DP_CUDA(cudaStreamSynchronize(c.stream));
+  klaunch(k_r_to_f32, g_nb(n), 256, 0, c.stream, (const double*)r, r32, c.scal, (int)G_IRR, n);
+  klaunch(k_z_from_f32_dot, red_grid(n), kRedThreads, 0, c.stream, (const float*)z32, z, (const double*)r, c.scal,
+          (int)G_IRR, (int)G_RZN, n, c.partial, c.counter);
+  klaunch(k_pcg_dir_g<double>, g_nb(n), 256, 0, c.stream, p, (const double*)z, Ap, n, (const double*)c.scal,
+          (int)G_RZN, (int)G_RZ, (const int*)&ctl->in_it);
+  klaunch(k_pcg_upd_check<double>, red_grid(n), kRedThreads, 0, c.stream, x, r, (const double*)p,
+          (const double*)Ap, n, c.scal, (int)G_RZ, (int)G_RZN, (int)G_PAP, (int)G_IRR, c.partial, c.counter,
+          (cudaGraphConditionalHandle)0, (DevCtl*)nullptr, 0);
+  DP_LAUNCH_CHECK();
 }
 
 // Captures the solve of c (on c.stream, which may be part of an enclosing

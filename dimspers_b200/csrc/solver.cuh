@@ -67,5 +67,6 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
 void to_cartesian(Ctx& c, const double* U, double* Uc);
 int schur_pcg_graph(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& res);
 void graph_free(Ctx& c);
+void profile_inner_vector_kernels(Ctx& c);
 
 }  // namespace dp

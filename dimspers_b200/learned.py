@@ -34,9 +34,16 @@ class GuessNet:
         dil = (C.c_int32 * layers)(*self.dilations)
         check(lib().dp_cnn_create(nrg, ntg, channels, layers, dil, max_batch, device, C.byref(self.h)))
         self.n = int(lib().dp_cnn_num_params(self.h))
+        self.bf16 = True
         self.x_mean = np.zeros(4, np.float32)
         self.x_std = np.ones(4, np.float32)
         self.y_mean, self.y_std = 0.0, 1.0
+
+    def set_math(self, bf16=True):
+        """BF16 tensor-core convolutions (FP32 accumulation; the default) or
+        FP32 CUDA-core convolutions."""
+        check(lib().dp_cnn_set_math(self.h, 1 if bf16 else 0))
+        self.bf16 = bool(bf16)
 
     def close(self):
         if self.h:

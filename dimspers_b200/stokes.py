@@ -350,7 +350,8 @@ class StokesContext:
     def profile_kernel(self, which, reps=50, flush_l2=False):
         """Average ms per launch: 0 FP32 A-apply, 1 FP64 A-apply, 2 V-cycle,
         3 stress post-processor, 4 viscosity update, 5 DEM tensor lookup, 6
-        thermal apply (last call's inputs);
+        thermal apply (last call's inputs), 7 the graph solve's inner-iteration
+        vector kernels launched outside the graph (for profilers);
         flush_l2 times each launch alone after overwriting 256 MB (cold L2)."""
         ms = C.c_double(0.0)
         self._chk(lib().dp_profile_kernel(self.h, int(which), int(reps), 1 if flush_l2 else 0, C.byref(ms)))

@@ -355,6 +355,12 @@ int dp_cnn_create(int32_t nrg, int32_t ntg, int32_t channels, int32_t layers, co
                   int32_t max_batch, int32_t device, dp_cnn** out);
 void dp_cnn_destroy(dp_cnn* net);
 int64_t dp_cnn_num_params(const dp_cnn* net);
+/* Arithmetic of the convolutions: bf16 = 1 (default) runs the forward pass and
+ * the data gradient as implicit GEMMs on the tensor cores (BF16 operands,
+ * FP32 accumulation; grids whose theta size is a multiple of 16), 0 runs all
+ * of them in FP32 on CUDA cores (the path checked against an FP64 reference).
+ * Weight gradients and Adam are FP32 either way (FP32 master weights). */
+int dp_cnn_set_math(dp_cnn* net, int32_t bf16);
 int dp_cnn_set_params(dp_cnn* net, const float* params, int64_t n);          /* host; resets Adam */
 int dp_cnn_get_params(dp_cnn* net, float* params, float* grads, int64_t n);   /* host; either may be NULL */
 int dp_cnn_forward(dp_cnn* net, const float* x, float* y, int32_t batch);
@@ -373,7 +379,9 @@ int dp_guess_from_grid(dp_ctx* ctx, const float* p_grid, int32_t nrg, int32_t nt
  * dp_stress call, 4 the viscosity update on the inputs of the last
  * dp_viscosity_arrhenius call, 5 the DEM tensor lookup on the inputs of the
  * last dp_anisotropic_tensor call, 6 the thermal element-by-element apply
- * (A p of the last dp_thermal_step's blocks).  flush_l2 = 0: `reps` back-to-back launches (warm L2);
+ * (A p of the last dp_thermal_step's blocks), 7 the vector kernels of one
+ * inner iteration of the graph solve launched outside the graph (for
+ * profilers; the event time includes their zeroing).  flush_l2 = 0: `reps` back-to-back launches (warm L2);
  * 1: a 256 MB buffer is read before each launch and each launch is timed
  * alone (cold L2, DRAM-bound figure). */
 int dp_profile_kernel(dp_ctx* ctx, int32_t which, int32_t reps, int32_t flush_l2, double* ms_per_launch);

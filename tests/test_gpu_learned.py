@@ -38,6 +38,7 @@ def test_network_gradients_match_torch_cpu():
     import torch
     nrg, ntg, C, L, dil = 6, 16, 8, 4, (1, 2, 3, 1)
     net = learned.GuessNet(nrg, ntg, C, L, dil, max_batch=2)
+    net.set_math(bf16=False)           # the FP32 CUDA-core path against FP64 torch
     net.init_params(seed=3)
     rng = np.random.default_rng(0)
     x = rng.standard_normal((2, 4, nrg, ntg)).astype(np.float32)
@@ -51,6 +52,81 @@ def test_network_gradients_match_torch_cpu():
     assert rel(yd.cpu().numpy(), y_ref) < 1e-5
     assert abs(loss - loss_ref) < 1e-5 * abs(loss_ref)
     assert rel(grads, g_ref) < 1e-4
+    net.close()
+
+
+def _bf16(a):
+    import torch
+    return torch.tensor(a, dtype=torch.float32).to(torch.bfloat16).to(torch.float64)
+
+
+def torch_forward_bf16(params, x, channels, layers, dil):
+    """The same network with every convolution operand rounded to BF16 (the
+    weights, and each layer's input activations) and exact accumulation: what
+    the tensor-core path computes, up to its FP32 accumulation order."""
+    import torch
+    import torch.nn.functional as F
+    p = torch.tensor(params, dtype=torch.float64)
+    h = torch.tensor(x, dtype=torch.float64)
+    off = 0
+    for l in range(layers):
+        cin = 4 if l == 0 else channels
+        cout = 1 if l == layers - 1 else channels
+        W = _bf16(p[off:off + cout * cin * 9].view(cout, cin, 3, 3).numpy())
+        off += cout * cin * 9
+        b = p[off:off + cout]
+        off += cout
+        d = dil[l]
+        hp = F.pad(_bf16(h.numpy()), (d, d, 0, 0), mode="circular")
+        hp = F.pad(hp, (0, 0, d, d))
+        h = F.conv2d(hp, W, b, dilation=d)
+        h = h.to(torch.float32).to(torch.float64)          # FP32 activations between layers
+        if l < layers - 1:
+            h = torch.relu(h)
+    return h.numpy()
+
+
+@pytest.mark.parametrize("channels", [16, 32])
+def test_tensor_core_forward_matches_bf16_reference(channels):
+    """BF16 operands, FP32 accumulation (mma.sync m16n8k16): equal to the
+    BF16-rounded network up to accumulation order, and within BF16 rounding
+    of the FP32 network."""
+    import torch
+    nrg, ntg, L, dil = 9, 48, 6, (1, 2, 4, 8, 3, 1)
+    net = learned.GuessNet(nrg, ntg, channels, L, dil, max_batch=2)
+    net.init_params(seed=5)
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal((2, 4, nrg, ntg)).astype(np.float32)
+    xd = torch.from_numpy(x).cuda()
+    y_tc = torch.empty((2, 1, nrg, ntg), dtype=torch.float32, device="cuda")
+    y_32 = torch.empty_like(y_tc)
+    net.forward(xd, y_tc)
+    net.set_math(bf16=False)
+    net.forward(xd, y_32)
+    ref = torch_forward_bf16(net.get_params(), x, channels, L, dil)
+    y_tc, y_32 = y_tc.cpu().numpy(), y_32.cpu().numpy()
+    assert rel(y_tc, ref) < 2e-4, rel(y_tc, ref)
+    assert 1e-5 < rel(y_tc, y_32) < 5e-2, rel(y_tc, y_32)
+    net.close()
+
+
+def test_tensor_core_gradients_close_to_fp32():
+    """Training gradients with the tensor-core forward and data gradient stay
+    within BF16 rounding of the FP32 path's."""
+    import torch
+    nrg, ntg, C, L, dil = 9, 32, 32, 6, (1, 2, 4, 8, 3, 1)
+    net = learned.GuessNet(nrg, ntg, C, L, dil, max_batch=2)
+    net.init_params(seed=4)
+    rng = np.random.default_rng(3)
+    x = torch.from_numpy(rng.standard_normal((2, 4, nrg, ntg)).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.standard_normal((2, 1, nrg, ntg)).astype(np.float32)).cuda()
+    loss_tc = net.gradients(x, t)
+    g_tc = net.get_params(grads=True)[1]
+    net.set_math(bf16=False)
+    loss_32 = net.gradients(x, t)
+    g_32 = net.get_params(grads=True)[1]
+    assert abs(loss_tc - loss_32) < 2e-2 * abs(loss_32)
+    assert rel(g_tc, g_32) < 5e-2, rel(g_tc, g_32)
     net.close()
 
 
