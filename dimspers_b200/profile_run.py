@@ -1,23 +1,28 @@
 """Launch every kernel family of the library once inside an NVTX range named
-"target", for per-kernel ncu captures.
+"target", for per-kernel ncu captures and launch lists.
 
-    python -m dimspers_b200.profile_run solve32 | solve64 | inner | post | cnn
+    python -m dimspers_b200.profile_run CASE [--nr 256 --nt 2048]
 
 Everything a case needs is set up outside the range (context, material,
 assembly or a first solve), so an ncu filter such as
 
     ncu --nvtx --nvtx-include "target/" --kernel-name-base demangled \\
         -k regex:'k_cheb_step<float>' -c 1 --clock-control none ... \\
-        python -m dimspers_b200.profile_run solve32
+        python -m dimspers_b200.profile_run vcycle
 
 captures the first launch of one kernel in the range.  The Stokes cases run on
-the 256x2048 fabric workload (1,048,576 elements: 327 MB of FP32 / 654 MB of
-FP64 element blocks, beyond the 126 MB L2, about 3 GB on the device):
+the fabric workload, by default at 256x2048 (1,048,576 elements: 327 MB of
+FP32 / 654 MB of FP64 element blocks, beyond the 126 MB L2, about 3 GB on the
+device):
 
-  solve32  assembly (FP32 blocks), one host-driven fast solve of 2 outer
-           iterations: FP32 multigrid (Galerkin levels, Gauss-Jordan coarse
-           inverse, Chebyshev, restriction, prolongation, dense coarsest),
-           the FP64 Krylov kernels, G and G^T, the compensated Schur kernels
+  apply32  one fine-level FP32 element-by-element A-apply
+  apply64  one fine-level FP64 A-apply
+  vcycle   one FP32 multigrid V-cycle from the fine level (after a solve built
+           the hierarchy): Chebyshev steps, restriction, prolongation, dense
+           coarsest, the coarse-level applies
+  solve32  assembly (FP32 blocks) and one host-driven fast solve of 2 outer
+           iterations: Galerkin levels, Gauss-Jordan coarse inverse, the
+           FP64 Krylov kernels, G and G^T, the compensated Schur kernels
   solve64  the same in FP64 with the lumped Schur preconditioner
   inner    the graph solve's inner-iteration vector kernels (launched outside
            the graph: ncu cannot look inside conditional graph nodes)
@@ -36,9 +41,12 @@ def _range(name):
     return torch.cuda.nvtx.range(name)
 
 
+SIZE = [256, 2048]
+
+
 def _stokes(precision):
     from . import StokesContext, inputs
-    nr, nt = 256, 2048
+    nr, nt = SIZE
     ctx = StokesContext(nr, nt, "discontinuous", pin_rotation=True)
     mat = inputs.make_material(ctx.mesh, "fabric", seed=1)
     ctx.set_material_ti(mat.eta_ip, mat.rho, mat.g, mat.delta, mat.dir_x, mat.dir_y)
@@ -54,6 +62,29 @@ def solve(precision):
         ctx.assemble(arm["precision"])
         ctx.solve(itmax=2, itmin=1, rtol=1e-30, inner_itmax=8, host_loop=1, raise_on_status=False, want_cart=False,
                   **arm)
+        torch.cuda.synchronize()
+    ctx.close()
+
+
+def apply(which):
+    import torch
+    ctx, arm = _stokes(1)
+    ctx.assemble(1 if which == 0 else 0)
+    torch.cuda.synchronize()
+    with _range("target"):
+        ctx.profile_kernel(which, reps=1)
+        torch.cuda.synchronize()
+    ctx.close()
+
+
+def vcycle():
+    import torch
+    ctx, arm = _stokes(1)
+    ctx.assemble(1)
+    ctx.solve(itmax=1, itmin=1, rtol=1e-30, inner_itmax=1, host_loop=1, raise_on_status=False, want_cart=False, **arm)
+    torch.cuda.synchronize()
+    with _range("target"):
+        ctx.profile_kernel(2, reps=1)
         torch.cuda.synchronize()
     ctx.close()
 
@@ -74,7 +105,7 @@ def post():
     from . import StokesContext, inputs
     from . import kernel_times as KT
     from .fabric import DEM
-    nr, nt = 256, 2048
+    nr, nt = SIZE
     c = StokesContext(nr, nt, "discontinuous")
     m = inputs.make_material(c.mesh, "aniso", seed=1)
     rng = np.random.default_rng(0)
@@ -118,7 +149,15 @@ def cnn():
     net.close()
 
 
-CASES = {"solve32": lambda: solve(1), "solve64": lambda: solve(0), "inner": inner, "post": post, "cnn": cnn}
+CASES = {"apply32": lambda: apply(0), "apply64": lambda: apply(1), "vcycle": vcycle, "solve32": lambda: solve(1),
+         "solve64": lambda: solve(0), "inner": inner, "post": post, "cnn": cnn}
 
 if __name__ == "__main__":
-    CASES[sys.argv[1]]()
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=sorted(CASES))
+    ap.add_argument("--nr", type=int, default=256)
+    ap.add_argument("--nt", type=int, default=2048)
+    a = ap.parse_args()
+    SIZE[:] = [a.nr, a.nt]
+    CASES[a.case]()
