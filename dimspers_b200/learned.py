@@ -18,7 +18,7 @@ from ._lib import DP_MEM_DEVICE, check, lib
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "weights")
-DEFAULT_ARCH = dict(channels=16, layers=6, dilations=(1, 2, 4, 8, 16, 1))
+DEFAULT_ARCH = dict(channels=32, layers=6, dilations=(1, 2, 4, 8, 16, 1))
 
 
 def grid_shape(nr_cells, ntheta_cells):
