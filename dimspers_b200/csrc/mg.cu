@@ -16,7 +16,8 @@
 // packed element-by-element form as the fine level.
 // Smoother: Chebyshev polynomial in D^-1 A (point Jacobi), bounds from a
 // 10-step CG-Lanczos estimate of lambda_max.  Coarsest level: assembled densely,
-// inverted once per setup by Gauss-Jordan sweeps and applied as a dense mat-vec.
+// inverted once per setup by block Gauss-Jordan (32 pivots per panel) and
+// applied as a dense mat-vec.
 #include <algorithm>
 #include <cmath>
 #include <stdexcept>
@@ -461,21 +462,70 @@ __global__ void k_dense_fix_diag(double* __restrict__ D, int n) {
   if (i < n && D[(size_t)i * n + i] == 0.0) D[(size_t)i * n + i] = 1.0;
 }
 
-// One Gauss-Jordan pivot step of the in-place inversion, ping-pong (A -> B):
-// with p = A_kk,  B_kk = 1/p,  B_kj = A_kj/p,  B_ik = -A_ik/p,
-// B_ij = A_ij - A_ik A_kj / p.  After the n steps B = A^-1.  The matrix is
-// SPD, so the pivots are positive and no pivoting is needed.  Threads run along
-// rows, so every step reads and writes the matrix with coalesced accesses.
-__global__ void k_gauss_jordan_step(const double* __restrict__ A, double* __restrict__ B, int n, int k) {
+// Block Gauss-Jordan inversion of the SPD coarsest matrix, one panel of up to
+// kGJPanel pivots K = [k0, k0 + b) at a time (no pivoting: the pivot blocks of an
+// SPD matrix are SPD).  With W = A_KK^-1 and T = A_{:,K} W, the panel step maps A
+// (old) to B (new):
+//   B_KK = W,   B_Kj = W A_Kj,   B_iK = -T_iK,   B_ij = A_ij - T_iK A_Kj
+// (i, j outside K).  After all panels B = A^-1.  Three launches per panel: the
+// pivot-block inverse (one CTA, shared memory), T (one thread per (row, pivot))
+// and the update (one thread per entry, coalesced along rows, ping-pong buffers).
+constexpr int kGJPanel = 32;
+
+__global__ void __launch_bounds__(kGJPanel * kGJPanel) k_gj_panel_inverse(const double* __restrict__ A,
+                                                                          double* __restrict__ W, int n, int k0,
+                                                                          int b) {
+  grid_dep_wait();
+  __shared__ double s[kGJPanel][kGJPanel + 1];
+  const int r = threadIdx.y, c = threadIdx.x;
+  s[r][c] = (r < b && c < b) ? A[(size_t)(k0 + r) * n + k0 + c] : (r == c ? 1.0 : 0.0);
+  __syncthreads();
+  for (int k = 0; k < b; ++k) {
+    const double ip = 1.0 / s[k][k];
+    const double akc = s[k][c], ark = s[r][k];
+    __syncthreads();                       // every read of pivot row/column before any write
+    double v;
+    if (r == k) v = (c == k) ? ip : akc * ip;
+    else if (c == k) v = -ark * ip;
+    else v = s[r][c] - ark * akc * ip;
+    s[r][c] = v;
+    __syncthreads();
+  }
+  W[r * kGJPanel + c] = s[r][c];
+}
+
+// T[i][m] = sum_l A[i][k0 + l] W[l][m]  (i < n, m < b; row stride kGJPanel)
+__global__ void k_gj_panel_cols(const double* __restrict__ A, const double* __restrict__ W, double* __restrict__ T,
+                                int n, int k0, int b) {
+  grid_dep_wait();
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)n * kGJPanel) return;
+  const int i = (int)(idx / kGJPanel), m = (int)(idx % kGJPanel);
+  double t = 0.0;
+  if (m < b)
+    for (int l = 0; l < b; ++l) t += A[(size_t)i * n + k0 + l] * W[l * kGJPanel + m];
+  T[idx] = t;
+}
+
+__global__ void k_gj_panel_update(const double* __restrict__ A, double* __restrict__ B, const double* __restrict__ W,
+                                  const double* __restrict__ T, int n, int k0, int b) {
   grid_dep_wait();
   const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (idx >= (int64_t)n * n) return;
   const int i = (int)(idx / n), j = (int)(idx % n);
-  const double ip = 1.0 / A[(size_t)k * n + k];
+  const bool ik = i >= k0 && i < k0 + b, jk = j >= k0 && j < k0 + b;
   double v;
-  if (i == k) v = (j == k) ? ip : A[(size_t)k * n + j] * ip;
-  else if (j == k) v = -A[(size_t)i * n + k] * ip;
-  else v = A[idx] - A[(size_t)i * n + k] * A[(size_t)k * n + j] * ip;
+  if (ik && jk) {
+    v = W[(i - k0) * kGJPanel + (j - k0)];
+  } else if (ik) {
+    v = 0.0;
+    for (int m = 0; m < b; ++m) v += W[(i - k0) * kGJPanel + m] * A[(size_t)(k0 + m) * n + j];
+  } else if (jk) {
+    v = -T[(size_t)i * kGJPanel + (j - k0)];
+  } else {
+    v = A[idx];
+    for (int m = 0; m < b; ++m) v -= T[(size_t)i * kGJPanel + m] * A[(size_t)(k0 + m) * n + j];
+  }
   B[idx] = v;
 }
 
@@ -777,11 +827,24 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
                                                                           (int)L.g.A(), (int)L.g.B(), n);
     klaunch(k_dense_fix_diag, (int)div_up(n, 256), 256, 0, c.stream, D, n);
     double* buf[2] = {D, Inv};
-    const int blocks = (int)div_up((int64_t)n * n, 256);
-    for (int k = 0; k < n; ++k) klaunch(k_gauss_jordan_step, blocks, 256, 0, c.stream, buf[k & 1], buf[(k + 1) & 1], n, k);
-    // step k writes buf[(k + 1) & 1]: for even n the inverse ends in D
-    if (!(n & 1)) DP_CUDA(cudaMemcpyAsync(Inv, D, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, c.stream));
+    double* W = nullptr;   // panel inverse (kGJPanel^2) and T (n x kGJPanel)
+    DP_CUDA(cudaMalloc(&W, sizeof(double) * (kGJPanel * kGJPanel + (size_t)n * kGJPanel)));
+    double* Tc = W + kGJPanel * kGJPanel;
+    const int npanel = (int)div_up(n, kGJPanel);
+    for (int p = 0; p < npanel; ++p) {
+      const int k0 = p * kGJPanel, b = std::min(kGJPanel, n - k0);
+      const double* Aold = buf[p & 1];
+      klaunch(k_gj_panel_inverse, 1, dim3(kGJPanel, kGJPanel), 0, c.stream, Aold, W, n, k0, b);
+      klaunch(k_gj_panel_cols, (int)div_up((int64_t)n * kGJPanel, 256), 256, 0, c.stream, Aold, (const double*)W, Tc,
+              n, k0, b);
+      klaunch(k_gj_panel_update, (int)div_up((int64_t)n * n, 256), 256, 0, c.stream, Aold, buf[(p + 1) & 1],
+              (const double*)W, (const double*)Tc, n, k0, b);
+    }
+    // panel p writes buf[(p + 1) & 1]: for an even panel count the inverse ends in D
+    if (!(npanel & 1)) DP_CUDA(cudaMemcpyAsync(Inv, D, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, c.stream));
     DP_LAUNCH_CHECK();
+    DP_CUDA(cudaStreamSynchronize(c.stream));
+    DP_CUDA(cudaFree(W));
   }
 }
 
