@@ -55,7 +55,7 @@ def main():
     for s in range(n):
         kind = "aniso" if s % 4 == 0 else "plumes"
         mat = inputs.make_material(mesh, kind, seed=1000 + s)
-        mats.append(mat)
+        mats.append(mat if s >= args.train else None)   # only the held-out materials are needed again
         ctx.set_material_ti(mat.eta_ip, mat.rho, mat.g, mat.delta, mat.dir_x, mat.dir_y)
         ctx.assemble(1)
         U, P, _, rep = ctx.solve(rtol=args.data_rtol, want_cart=False, **solve_opts)
