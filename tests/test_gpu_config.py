@@ -23,6 +23,8 @@ What the oracle itself achieves sets the bars (tests/golden/tight.json):
 Tolerances:
   FP64 path, rtol 1e-12 vs yardstick   U, P <= 2e-9          (oracle floor 4.3e-10)
   either path, rtol 1e-8 vs yardstick  <= 3 x the oracle's own rtol-1e-8 error
+                                       (config 1: ~5e-6 U, ~1.5e-5 P; 128x1024: 3.9e-5 U,
+                                       9.0e-4 P)
   fast path, rtol 1e-11 vs yardstick   U, P <= 1e-7          (the fast-path bar)
 """
 import json
@@ -133,10 +135,12 @@ def test_aniso128_both_arms_at_reference_rule(aniso128):
     """At rtol 1e-8 the plain FP64 arm sits ~1e-5 from the yardstick (the
     problem's own floor, as on config 1); the fast arm is no further off."""
     ctx, fx = aniso128
+    own = META["tight128"]["oracle_rtol1e-8_lumped_vs_tight"]   # the oracle's own rtol-1e-8 error
     U, P, rep = _solve(ctx, PLAIN, rtol=1e-8)
     eu64, ep64 = _err_sub(U, P, fx)
-    print(f"128x1024 FP64 rtol1e-8: U {eu64:.2e} P {ep64:.2e}; outer {rep['iterations']}")
-    assert eu64 <= 1e-4 and ep64 <= 1e-3, (eu64, ep64)
+    print(f"128x1024 FP64 rtol1e-8: U {eu64:.2e} P {ep64:.2e} (oracle at rtol 1e-8: U {own['u']:.1e} "
+          f"P {own['p']:.1e}); outer {rep['iterations']}")
+    assert eu64 <= 3 * own["u"] and ep64 <= 3 * own["p"], (eu64, ep64, own)
     U, P, rep = _solve(ctx, FAST, rtol=1e-8)
     eu, ep = _err_sub(U, P, fx)
     print(f"128x1024 fast rtol1e-8: U {eu:.2e} P {ep:.2e}; outer {rep['iterations']}")
