@@ -486,7 +486,7 @@ int dp_ctx_create(const dp_mesh_desc* d, dp_ctx** out) {
     dalloc(&c.scal, 64);
     DP_CUDA(cudaMemset(c.scal, 0, sizeof(double) * 64));
     DP_CUDA(cudaMallocHost((void**)&c.h_scal, sizeof(double) * 64));
-    dalloc(&c.partial, 4 * 1024);
+    dalloc(&c.partial, kPartialDoubles);
     dalloc(&c.counter, 1);
     DP_CUDA(cudaMemset(c.counter, 0, sizeof(unsigned int)));
     c.work.assign(W_COUNT, nullptr);

@@ -90,14 +90,16 @@ __global__ void k_ref_check(cudaGraphConditionalHandle h, DevCtl* ctl, const dou
 // use_ref: the stopping tolerance is relative to the zero-guess residual
 // ||r(P = 0)|| (learned-guess mode), so a guess shortens the solve only by
 // starting closer to the same absolute target.
+// A non-finite initial residual (a failed initial inner solve) is a breakdown,
+// not a zero right-hand side.
 __global__ void k_outer_init(cudaGraphConditionalHandle h, DevCtl* ctl, const double* scal, int use_ref) {
   grid_dep_wait();
   const double r0 = use_ref ? ctl->r0ref : sqrt(scal[S_RR]);
   ctl->r0 = r0;
   ctl->tol = r0 * ctl->rtol;
   ctl->outer_it = 0;
-  ctl->status = r0 > 0.0 ? 1 : 0;
-  cudaGraphSetConditional(h, (r0 > 0.0 && ctl->itmax >= 1) ? 1u : 0u);
+  ctl->status = !isfinite(r0) || !isfinite(scal[S_RR]) ? 2 : (r0 > 0.0 ? 1 : 0);
+  cudaGraphSetConditional(h, (ctl->status == 1 && ctl->itmax >= 1) ? 1u : 0u);
 }
 
 __global__ void k_outer_check(cudaGraphConditionalHandle h, DevCtl* ctl, const double* scal) {
@@ -132,11 +134,11 @@ __global__ void k_outer_start(DevCtl* ctl, const double* scal, int use_ref) {
   ctl->tol = r0 * ctl->rtol;
   ctl->outer_it = 0;
   ctl->restarts = 0;
-  ctl->status = r0 > 0.0 ? 1 : 0;
+  ctl->status = !isfinite(r0) || !isfinite(scal[S_RR]) ? 2 : (r0 > 0.0 ? 1 : 0);
 }
 __global__ void k_restart_init(cudaGraphConditionalHandle h, const DevCtl* ctl) {
   grid_dep_wait();
-  cudaGraphSetConditional(h, (ctl->r0 > 0.0 && ctl->itmax >= 1) ? 1u : 0u);
+  cudaGraphSetConditional(h, (ctl->status == 1 && ctl->itmax >= 1) ? 1u : 0u);
 }
 // outer loop (re)entry: continue while the current (true) residual misses the tolerance
 __global__ void k_outer_resume(cudaGraphConditionalHandle h, DevCtl* ctl, const double* scal) {
@@ -194,7 +196,7 @@ template <typename T>
 __global__ void k_pcg_dir_g(T* __restrict__ p, const T* __restrict__ z, T* __restrict__ Ap, int64_t n,
                             const double* scal, int rzn, int rz, const int* it) {
   grid_dep_wait();
-  const double beta = (*it == 0) ? 0.0 : scal[rzn] / scal[rz];
+  const double beta = (*it == 0 || scal[rz] == 0.0) ? 0.0 : scal[rzn] / scal[rz];
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) {
     p[i] = (T)((double)z[i] + beta * (double)p[i]);
@@ -251,7 +253,11 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_upd_check(T* __restrict__ x
                                                                 int irr, double* partial, unsigned int* counter,
                                                                 cudaGraphConditionalHandle h, DevCtl* ctl, int fp32) {
   grid_dep_wait();
-  const double alpha = scal[rzn] / scal[pap];
+  // a non-positive or non-finite p.Ap (breakdown, e.g. an FP32 operator that
+  // rounding made indefinite) leaves x and r unchanged and ends the loop
+  const double pap_v = scal[pap];
+  const bool ok = pap_v > 0.0 && isfinite(pap_v) && isfinite(scal[rzn]);
+  const double alpha = ok ? scal[rzn] / pap_v : 0.0;
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
     x[i] += (T)(alpha * (double)p[i]);
@@ -268,7 +274,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_upd_check(T* __restrict__ x
     else { it = ++ctl->in_it; tol2 = ctl->in_tol2; ctl->in_total += 1; }
     scal[rz] = scal[rzn];
     const double rr = scal[irr];
-    const bool go = isfinite(rr) && rr > tol2 && it < ctl->inner_itmax;
+    const bool go = ok && isfinite(rr) && rr > tol2 && it < ctl->inner_itmax;
     cudaGraphSetConditional(h, go ? 1u : 0u);
   }
 }

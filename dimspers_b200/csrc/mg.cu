@@ -287,22 +287,31 @@ __global__ void k_prolong_add(const T* __restrict__ xc, T* __restrict__ xf, T* _
   grid_dep_wait();
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= Af * Bf) return;
-  const int a = n % Af, b = n / Af;
+  const int b = n / Af, a = n - b * Af;
   int cn[6];
   double w[6];
   fine_node_weights(a, b, ncrc, Ac, Bc, cn, w);
-  double s0 = 0.0, s1 = 0.0;
+  // the 6 nodes of the containing coarse element are always valid: gather them
+  // all unconditionally (zero weights included) so the loads issue together
+  typedef typename V2<T>::T X2;
+  const X2* xc2 = reinterpret_cast<const X2*>(xc);
+  X2 v[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) v[k] = xc2[cn[k]];
+  X2 xv = reinterpret_cast<const X2*>(xf)[n];
+  T s0 = (T)0, s1 = (T)0;
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
-    if (w[k] != 0.0) {
-      s0 += w[k] * (double)xc[2 * cn[k]];
-      s1 += w[k] * (double)xc[2 * cn[k] + 1];
-    }
+    s0 += (T)w[k] * v[k].x;
+    s1 += (T)w[k] * v[k].y;
   }
-  if (!dof_fixed(a, b, 0, Af - 1, pin)) xf[2 * n] += (T)s0;
-  if (!dof_fixed(a, b, 1, Af - 1, pin)) xf[2 * n + 1] += (T)s1;
-  zb[2 * n] = (T)0;
-  zb[2 * n + 1] = (T)0;
+  if (!dof_fixed(a, b, 0, Af - 1, pin)) xv.x += s0;
+  if (!dof_fixed(a, b, 1, Af - 1, pin)) xv.y += s1;
+  X2 zero;
+  zero.x = (T)0;
+  zero.y = (T)0;
+  reinterpret_cast<X2*>(xf)[n] = xv;
+  reinterpret_cast<X2*>(zb)[n] = zero;
 }
 
 // bc = P^T (r - t) per coarse node (gather over the class stencil); constrained
@@ -373,9 +382,99 @@ __global__ void __launch_bounds__(256) k_restrict_g(const T* __restrict__ r, con
   }
 }
 
+// Tiled form of the same restriction for the large levels.  One CTA = 16 x 16
+// coarse nodes; the fine values r - t of the CTA's stencil footprint (a 39 x 39
+// patch of fine nodes, constrained fine DOFs zeroed) are read from global
+// memory once into shared memory, and each coarse node gathers its class
+// stencil from there (the gather form reads every fine value ~4 times through
+// L2).  Warps are class-uniform (64 coarse nodes of each parity class), so the
+// stencil table reads are constant-cache broadcasts.  Arithmetic in the level's
+// precision (the stencil weights are dyadic fractions, exact in FP32).
+constexpr int kRTile = 16;
+constexpr int kRPatch = 2 * (kRTile - 1) + 1 + 8;   // 39: stencil offsets reach 4 fine nodes each way
+template <typename T>
+__global__ void __launch_bounds__(256) k_restrict_tile(const T* __restrict__ r, const T* __restrict__ t,
+                                                       T* __restrict__ bc, int Af, int Bf, int Ac, int Bc, int pin,
+                                                       int first, const T* __restrict__ dinv_c, T* __restrict__ xc,
+                                                       T* __restrict__ rc, T* __restrict__ dc, T* __restrict__ tc,
+                                                       const double* __restrict__ coef_c) {
+  grid_dep_wait();
+  typedef typename V2<T>::T X2;
+  __shared__ X2 sp[kRPatch][kRPatch + 1];    // [b][a]
+  const int ac0 = blockIdx.x * kRTile, bc0 = blockIdx.y * kRTile;
+  const int fa0 = 2 * ac0 - 4, fb0 = 2 * bc0 - 4;
+  const X2* r2 = reinterpret_cast<const X2*>(r);
+  const X2* t2 = reinterpret_cast<const X2*>(t);
+  for (int k = threadIdx.x; k < kRPatch * kRPatch; k += blockDim.x) {
+    const int la = k % kRPatch, lb = k / kRPatch;
+    const int a = fa0 + la;
+    int b = fb0 + lb;
+    b += (b < 0) ? Bf : 0;                   // the patch reaches at most 4 nodes past either end
+    b -= (b >= Bf) ? Bf : 0;
+    X2 v;
+    v.x = (T)0;
+    v.y = (T)0;
+    if (a >= 0 && a < Af) {
+      const int64_t f = a + (int64_t)Af * b;
+      const X2 rv = r2[f], tv = t2[f];
+      if (!dof_fixed(a, b, 0, Af - 1, pin)) v.x = rv.x - tv.x;
+      if (!dof_fixed(a, b, 1, Af - 1, pin)) v.y = rv.y - tv.y;
+    }
+    sp[lb][la] = v;
+  }
+  __syncthreads();
+  const int cls = threadIdx.x >> 6, loc = threadIdx.x & 63;
+  const int pa = cls & 1, pb = cls >> 1;
+  const int ac = ac0 + 2 * (loc & 7) + pa, bcn = bc0 + 2 * (loc >> 3) + pb;
+  if (ac >= Ac || bcn >= Bc) return;
+  const int m = c_rtab.n[cls];
+  T s0 = (T)0, s1 = (T)0;
+  for (int j = 0; j < m; ++j) {
+    const int la = 2 * (ac - ac0) + 4 + c_rtab.da[cls][j];
+    const int lb = 2 * (bcn - bc0) + 4 + c_rtab.db[cls][j];
+    const X2 v = sp[lb][la];
+    const T w = (T)c_rtab.w[cls][j];
+    s0 += w * v.x;
+    s1 += w * v.y;
+  }
+  const int n = ac + Ac * bcn;
+  const T b0 = dof_fixed(ac, bcn, 0, Ac - 1, pin) ? (T)0 : s0;
+  const T b1 = dof_fixed(ac, bcn, 1, Ac - 1, pin) ? (T)0 : s1;
+  X2 bv;
+  bv.x = b0;
+  bv.y = b1;
+  reinterpret_cast<X2*>(bc)[n] = bv;
+  if (first) {
+    const T it = (T)coef_c[0];
+    T z0, z1;
+    const T a = dinv_c[3 * (int64_t)n], bb = dinv_c[3 * (int64_t)n + 1], c = dinv_c[3 * (int64_t)n + 2];
+    z0 = a * b0 + bb * b1;
+    z1 = bb * b0 + c * b1;
+    X2 zero, dv;
+    zero.x = (T)0;
+    zero.y = (T)0;
+    dv.x = it * z0;
+    dv.y = it * z1;
+    reinterpret_cast<X2*>(tc)[n] = zero;
+    reinterpret_cast<X2*>(rc)[n] = bv;
+    reinterpret_cast<X2*>(dc)[n] = dv;
+    reinterpret_cast<X2*>(xc)[n] = dv;
+  }
+}
+
 // ---- Chebyshev smoother vector steps (per node, coefficients read from device) --
 // first step from x = 0: r = b, d = (1/theta) D^-1 b, x = d
 // (every Chebyshev kernel also zeroes t, which the next apply accumulates into)
+// The three kernels compute in the precision of the level (FP32 on the FP32
+// hierarchy) and move each node's pair of components with one 8/16-byte
+// access, all loads issued before the arithmetic.
+template <typename T>
+__device__ __forceinline__ void bj_apply_t(const T* __restrict__ dinv, int64_t n, T r0, T r1, T& z0, T& z1) {
+  const T a = dinv[3 * n], b = dinv[3 * n + 1], c = dinv[3 * n + 2];
+  z0 = a * r0 + b * r1;
+  z1 = b * r0 + c * r1;
+}
+
 template <typename T>
 __global__ void k_cheb_first(const T* __restrict__ b, const T* __restrict__ dinv, T* __restrict__ x,
                              T* __restrict__ r, T* __restrict__ d, T* __restrict__ t, const double* __restrict__ coef,
@@ -383,14 +482,18 @@ __global__ void k_cheb_first(const T* __restrict__ b, const T* __restrict__ dinv
   grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
-  t[2 * n] = (T)0; t[2 * n + 1] = (T)0;
-  const double it = coef[0];
-  const double b0 = (double)b[2 * n], b1 = (double)b[2 * n + 1];
-  double z0, z1;
-  bj_apply<T>(dinv, n, b0, b1, z0, z1);
-  r[2 * n] = (T)b0; r[2 * n + 1] = (T)b1;
-  d[2 * n] = (T)(it * z0); d[2 * n + 1] = (T)(it * z1);
-  x[2 * n] = (T)(it * z0); x[2 * n + 1] = (T)(it * z1);
+  typedef typename V2<T>::T X2;
+  const X2 bv = reinterpret_cast<const X2*>(b)[n];
+  const T it = (T)coef[0];
+  T z0, z1;
+  bj_apply_t<T>(dinv, n, bv.x, bv.y, z0, z1);
+  X2 zero, dv;
+  zero.x = (T)0; zero.y = (T)0;
+  dv.x = it * z0; dv.y = it * z1;
+  reinterpret_cast<X2*>(t)[n] = zero;
+  reinterpret_cast<X2*>(r)[n] = bv;
+  reinterpret_cast<X2*>(d)[n] = dv;
+  reinterpret_cast<X2*>(x)[n] = dv;
 }
 // first step from a given x: r = b - Ax (Ax in r on entry), d = (1/theta) D^-1 r, x += d
 template <typename T>
@@ -400,31 +503,48 @@ __global__ void k_cheb_first_x(const T* __restrict__ b, const T* __restrict__ di
   grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
-  t[2 * n] = (T)0; t[2 * n + 1] = (T)0;
-  const double it = coef[0];
-  const double r0 = (double)b[2 * n] - (double)r[2 * n], r1 = (double)b[2 * n + 1] - (double)r[2 * n + 1];
-  double z0, z1;
-  bj_apply<T>(dinv, n, r0, r1, z0, z1);
-  r[2 * n] = (T)r0; r[2 * n + 1] = (T)r1;
-  d[2 * n] = (T)(it * z0); d[2 * n + 1] = (T)(it * z1);
-  x[2 * n] += (T)(it * z0); x[2 * n + 1] += (T)(it * z1);
+  typedef typename V2<T>::T X2;
+  const X2 bv = reinterpret_cast<const X2*>(b)[n];
+  const X2 av = reinterpret_cast<const X2*>(r)[n];
+  const X2 xv = reinterpret_cast<const X2*>(x)[n];
+  const T it = (T)coef[0];
+  X2 rv, dv, zero;
+  rv.x = bv.x - av.x; rv.y = bv.y - av.y;
+  T z0, z1;
+  bj_apply_t<T>(dinv, n, rv.x, rv.y, z0, z1);
+  dv.x = it * z0; dv.y = it * z1;
+  zero.x = (T)0; zero.y = (T)0;
+  reinterpret_cast<X2*>(t)[n] = zero;
+  reinterpret_cast<X2*>(r)[n] = rv;
+  reinterpret_cast<X2*>(d)[n] = dv;
+  X2 xn;
+  xn.x = xv.x + dv.x; xn.y = xv.y + dv.y;
+  reinterpret_cast<X2*>(x)[n] = xn;
 }
-// r -= Ad; d = c1 d + c2 D^-1 r; x += d  (c1, c2 = coef[0], coef[1])
+// r -= Ad; d = c1 d + c2 D^-1 r; x += d  (c1, c2 = coef[0], coef[1]); Ad = 0 for the next apply
 template <typename T>
 __global__ void k_cheb_step(T* __restrict__ Ad, const T* __restrict__ dinv, T* __restrict__ x,
                             T* __restrict__ r, T* __restrict__ d, const double* __restrict__ coef, int64_t nnod) {
   grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
-  const double c1 = coef[0], c2 = coef[1];
-  const double r0 = (double)r[2 * n] - (double)Ad[2 * n], r1 = (double)r[2 * n + 1] - (double)Ad[2 * n + 1];
-  Ad[2 * n] = (T)0; Ad[2 * n + 1] = (T)0;
-  double z0, z1;
-  bj_apply<T>(dinv, n, r0, r1, z0, z1);
-  const double d0 = c1 * (double)d[2 * n] + c2 * z0, d1 = c1 * (double)d[2 * n + 1] + c2 * z1;
-  r[2 * n] = (T)r0; r[2 * n + 1] = (T)r1;
-  d[2 * n] = (T)d0; d[2 * n + 1] = (T)d1;
-  x[2 * n] += (T)d0; x[2 * n + 1] += (T)d1;
+  typedef typename V2<T>::T X2;
+  const X2 av = reinterpret_cast<const X2*>(Ad)[n];
+  const X2 rv = reinterpret_cast<const X2*>(r)[n];
+  const X2 dv = reinterpret_cast<const X2*>(d)[n];
+  const X2 xv = reinterpret_cast<const X2*>(x)[n];
+  const T c1 = (T)coef[0], c2 = (T)coef[1];
+  X2 rn, dn, xn, zero;
+  rn.x = rv.x - av.x; rn.y = rv.y - av.y;
+  T z0, z1;
+  bj_apply_t<T>(dinv, n, rn.x, rn.y, z0, z1);
+  dn.x = c1 * dv.x + c2 * z0; dn.y = c1 * dv.y + c2 * z1;
+  xn.x = xv.x + dn.x; xn.y = xv.y + dn.y;
+  zero.x = (T)0; zero.y = (T)0;
+  reinterpret_cast<X2*>(Ad)[n] = zero;
+  reinterpret_cast<X2*>(r)[n] = rn;
+  reinterpret_cast<X2*>(d)[n] = dn;
+  reinterpret_cast<X2*>(x)[n] = xn;
 }
 // z = D^-1 r (nodal blocks)
 template <typename T>
@@ -527,6 +647,20 @@ __global__ void k_gj_panel_update(const double* __restrict__ A, double* __restri
     for (int m = 0; m < b; ++m) v -= T[(size_t)i * kGJPanel + m] * A[(size_t)(k0 + m) * n + j];
   }
   B[idx] = v;
+}
+
+// A = (A + A^T) / 2 in place (one thread per pair i < j): the inverse of the SPD
+// coarse matrix is symmetric in exact arithmetic; the elimination's rounding is
+// not, and a symmetric coarse solve keeps the V-cycle a symmetric preconditioner.
+__global__ void k_symmetrize(double* __restrict__ A, int n) {
+  grid_dep_wait();
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)n * n) return;
+  const int i = (int)(idx / n), j = (int)(idx % n);
+  if (i >= j) return;
+  const double v = 0.5 * (A[(size_t)i * n + j] + A[(size_t)j * n + i]);
+  A[(size_t)i * n + j] = v;
+  A[(size_t)j * n + i] = v;
 }
 
 // x = Inv b, one CTA per row: each thread reads a few entries of the row (all
@@ -842,6 +976,7 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
     }
     // panel p writes buf[(p + 1) & 1]: for an even panel count the inverse ends in D
     if (!(npanel & 1)) DP_CUDA(cudaMemcpyAsync(Inv, D, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, c.stream));
+    klaunch(k_symmetrize, (int)div_up((int64_t)n * n, 256), 256, 0, c.stream, Inv, n);
     DP_LAUNCH_CHECK();
     DP_CUDA(cudaStreamSynchronize(c.stream));
     DP_CUDA(cudaFree(W));
@@ -914,11 +1049,19 @@ static void vcycle(Ctx& c, size_t l, const T* b, T* x, const MGOptions& o, bool 
   launch_apply_K_acc<T, T>(L.g, level_K<T>(L), (const T*)L.d, t, c.stream);
   const bool fuse = !(l + 2 == c.mg.size() && dense_coarsest);
   const int nA0 = (int)((C.g.A() + 1) >> 1);  // coarse nodes per parity class (upper bound)
-  const bool small = C.g.nnod < 32768;
-  dim3 grid((unsigned)div_up((small ? 4 : 1) * (int64_t)nA0 * (C.g.B() >> 1), 256), 4);
-  klaunch(small ? k_restrict_g<T, 4> : k_restrict_g<T, 1>, grid, 256, 0, c.stream, (const T*)r, (const T*)t, bc, (int)L.g.A(), (int)L.g.B(),
-          (int)C.g.A(), (int)C.g.B(), C.g.pin, fuse ? 1 : 0, (const T*)level_dinv<T>(C), xc, (T*)C.r, (T*)C.d,
-          (T*)C.t, (const double*)C.cheb);
+  // the tiled form needs whole tiles along theta (its patch then wraps at most once)
+  const bool small = C.g.nnod < 32768 || C.g.B() % kRTile != 0;
+  if (small) {
+    dim3 grid((unsigned)div_up(4 * (int64_t)nA0 * (C.g.B() >> 1), 256), 4);
+    klaunch(k_restrict_g<T, 4>, grid, 256, 0, c.stream, (const T*)r, (const T*)t, bc, (int)L.g.A(), (int)L.g.B(),
+            (int)C.g.A(), (int)C.g.B(), C.g.pin, fuse ? 1 : 0, (const T*)level_dinv<T>(C), xc, (T*)C.r, (T*)C.d,
+            (T*)C.t, (const double*)C.cheb);
+  } else {
+    dim3 grid((unsigned)div_up(C.g.A(), kRTile), (unsigned)div_up(C.g.B(), kRTile));
+    klaunch(k_restrict_tile<T>, grid, 256, 0, c.stream, (const T*)r, (const T*)t, bc, (int)L.g.A(), (int)L.g.B(),
+            (int)C.g.A(), (int)C.g.B(), C.g.pin, fuse ? 1 : 0, (const T*)level_dinv<T>(C), xc, (T*)C.r, (T*)C.d,
+            (T*)C.t, (const double*)C.cheb);
+  }
   DP_LAUNCH_CHECK();
   vcycle<T>(c, l + 1, bc, xc, o, fuse);
   klaunch(k_prolong_add<T>, tpb(L.g.nnod), 256, 0, c.stream, xc, x, r, (int)L.g.A(), (int)L.g.B(), C.g.ncr, (int)C.g.A(),

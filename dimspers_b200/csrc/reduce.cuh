@@ -10,8 +10,11 @@
 
 namespace dp {
 
-constexpr int kRedBlocks = 592;   // 4 x 148 SMs
+constexpr int kRedBlocks = 1184;  // 8 x 148 SMs: 64 resident warps per SM keep enough loads in flight
 constexpr int kRedThreads = 256;
+// per-context partials: room for two double-double values (4 doubles) per block
+constexpr int kPartialDoubles = 8 * 1024;
+static_assert(4 * kRedBlocks <= kPartialDoubles, "reduction partial buffer too small for the grid");
 
 __device__ inline double warp_sum(double v) {
 #pragma unroll

@@ -195,7 +195,8 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_update(T* __restrict__ x, T
                                                              const T* __restrict__ Ap, int64_t n, double* scal, int rz_slot,
                                                              double* partial, unsigned int* counter) {
   grid_dep_wait();
-  const double alpha = scal[rz_slot] / scal[S_PAP];
+  const double pap = scal[S_PAP];
+  const double alpha = (pap > 0.0 && isfinite(pap)) ? scal[rz_slot] / pap : 0.0;   // breakdown: no update
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
     x[i] += (T)(alpha * (double)p[i]);
@@ -469,6 +470,13 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
   DP_LAUNCH_CHECK();
   const double r0 = std::sqrt(read_slot(c, S_RR));
   res.r0 = r0;
+  if (!std::isfinite(r0)) {   // the initial inner solve failed: breakdown, not a zero residual
+    res.status = 2;
+    res.iterations = 0;
+    res.relres = r0;
+    res.inner_its = st.its;
+    return res.status;
+  }
   const double tol = r0 * cfg.rtol;
   // d = r .* pc (or M^-1 r); q = d
   if (cfg.schur_pc == 1) {
