@@ -26,7 +26,7 @@ fp64_same_algorithm
             learned guess); value / this = the gain of the precision pattern
 secondary   the 128x1024 anisotropic workload: both arms, and their errors
             against the tightly converged FP64 oracle solution committed in
-            tests/golden (the yardstick), plus the fast arm at tighter rtol
+            tests/golden (the yardstick), plus the fast arm at rtol 1e-9..1e-12
 roofline    the fine-level FP32 element-by-element A-apply, the dominant kernel
 cpu_baseline  the reference's CPU algorithm (the FP64 oracle) by a cost model
             fitted on oracle solves of two smaller meshes (oracle.refmodel)
@@ -391,7 +391,7 @@ def run_secondary(local, barrier, host_loop):
         out["fast_err_vs_tight"] = err_vs_fixture(Uf, Pf, fx)
         out["fp64_err_vs_tight"] = err_vs_fixture(U64, P64, fx)
         sweep = []
-        for rt in (1e-9, 1e-10, 1e-11):
+        for rt in (1e-9, 1e-10, 1e-11, 1e-12):
             ms_t, rep_t = w.timed(FAST, 0, 1, barrier, rtol=rt, inner_rtol=min(1e-10, rt * 1e-2), relax_base=rt)
             Ut, Pt = w.solution()
             e = err_vs_fixture(Ut, Pt, fx)

@@ -456,7 +456,17 @@ int schur_pcg(Ctx& c, const SolveCfg& cfg, double* U, double* P, SolveResult& re
   InnerStats st;
 
   // Rhs = F + G P ; U = K^-1 Rhs   (IterativeSolvers.jl:101-111)
-  if (!cfg.use_guess) DP_CUDA(cudaMemsetAsync(P, 0, sizeof(double) * nP, c.stream));
+  // Pressure gauge: constant pressure is in the null space of G under free slip,
+  // so P is defined up to a constant.  StokesPcCG starts from P = 0 and adds
+  // only mean-free directions (IterativeSolvers.jl:101, rm0space! of q), so its
+  // P has zero mean; a given initial P (a guess) has its mean removed first so
+  // that the answer carries the same gauge.  It changes nothing else (G 1 = 0).
+  if (!cfg.use_guess) {
+    DP_CUDA(cudaMemsetAsync(P, 0, sizeof(double) * nP, c.stream));
+  } else {
+    launch_sum_c(c, P, nP, S_TMP2);
+    klaunch(k_sub_mean, nb256(nP), 256, 0, c.stream, P, nP, (const double*)(c.scal + S_TMP2));
+  }
   launch_apply_G(c, P, y);
   klaunch(k_add, nb256(nU), 256, 0, c.stream, c.F, y, rhs, nU);
   DP_LAUNCH_CHECK();
