@@ -330,11 +330,69 @@ __global__ void k_apply_GT(const double* __restrict__ G, const double* __restric
   }
 }
 
+// y = G p with the scatter pre-summed per warp: with ncr a multiple of 16 the 32
+// elements of a warp are the two triangles of 16 consecutive cells of one theta
+// column, which share 33 x 3 = 99 lattice nodes.  The warp adds its 384 values
+// into a shared-memory copy of those nodes first and then issues one global FP64
+// atomic per node and component (198), since sm_100a has no vector FP64 reduction.
+constexpr int kGWarpNodes = 99;
+__global__ void __launch_bounds__(128) k_apply_G_warp(const double* __restrict__ G, const double* __restrict__ p,
+                                                      double* __restrict__ y, int nel, int ncr, int nct, int A, int B,
+                                                      int pressure) {
+  grid_dep_wait();
+  __shared__ double acc[4][2 * kGWarpNodes];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e0 = e - lane;                        // first element of the warp (nel is a multiple of 32)
+  if (e0 >= nel) return;                          // whole warps past the last element (tail block)
+  const int q0 = e0 >> 1, ir0 = q0 % ncr, it = q0 / ncr;
+  double* s = acc[w];
+  for (int k = lane; k < 2 * kGWarpNodes; k += 32) s[k] = 0.0;
+  __syncwarp();
+  {
+    const int q = e >> 1, t = e & 1;
+    const int ir = q % ncr;
+    int pd[3];
+    element_pdofs_dev(e, ncr, nct, pressure, pd);
+    const double p0 = p[pd[0]], p1 = p[pd[1]], p2 = p[pd[2]];
+    // local lattice offsets (a relative to 2 ir0, b relative to 2 it) of the 6 nodes
+    const int la0 = 2 * (ir - ir0);
+    int la[6], lb[6];
+    if (t == 0) {
+      la[0] = la0; la[1] = la0; la[2] = la0 + 2; la[3] = la0; la[4] = la0 + 1; la[5] = la0 + 1;
+      lb[0] = 0; lb[1] = 2; lb[2] = 0; lb[3] = 1; lb[4] = 1; lb[5] = 0;
+    } else {
+      la[0] = la0; la[1] = la0 + 2; la[2] = la0 + 2; la[3] = la0 + 1; la[4] = la0 + 2; la[5] = la0 + 1;
+      lb[0] = 2; lb[1] = 2; lb[2] = 0; lb[3] = 2; lb[4] = 1; lb[5] = 1;
+    }
+#pragma unroll
+    for (int d = 0; d < 12; ++d) {
+      const double v = G[(size_t)d * nel + e] * p0 + G[(size_t)(12 + d) * nel + e] * p1 +
+                       G[(size_t)(24 + d) * nel + e] * p2;
+      const int k = d >> 1;
+      atomicAdd(&s[2 * (la[k] + 33 * lb[k]) + (d & 1)], v);
+    }
+  }
+  __syncwarp();
+  for (int k = lane; k < kGWarpNodes; k += 32) {
+    const int a = 2 * ir0 + k % 33, bl = 2 * it + k / 33;
+    const int64_t n = a + (int64_t)A * (bl >= B ? bl - B : bl);
+    atomicAdd(&y[2 * n], s[2 * k]);
+    atomicAdd(&y[2 * n + 1], s[2 * k + 1]);
+  }
+}
+
 void launch_apply_G(Ctx& c, const double* p, double* y) {
   const Level& L = c.fine;
   DP_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * 2 * L.nnod, c.stream));
-  klaunch(k_apply_G, (int)div_up(L.nel, 128), 128, 0, c.stream, c.Gp, p, y, (int)L.nel, L.ncr, L.nct, (int)L.A(),
-                                                           (int)L.B(), c.mesh.pressure);
+  if (L.ncr % 16 == 0) {
+    // nel = 2 ncr nct is then a multiple of 32 and every warp is whole
+    klaunch(k_apply_G_warp, (int)div_up(L.nel, 128), 128, 0, c.stream, c.Gp, p, y, (int)L.nel, L.ncr, L.nct,
+            (int)L.A(), (int)L.B(), c.mesh.pressure);
+  } else {
+    klaunch(k_apply_G, (int)div_up(L.nel, 128), 128, 0, c.stream, c.Gp, p, y, (int)L.nel, L.ncr, L.nct, (int)L.A(),
+            (int)L.B(), c.mesh.pressure);
+  }
   DP_LAUNCH_CHECK();
 }
 
