@@ -74,7 +74,10 @@ typedef struct {
                               StokesPcCG_pardiso keeps U, P); 2: learned guess:
                               start from the P passed in only if its Schur
                               residual is below the zero guess's, and stop at
-                              rtol relative to the zero-guess residual       */
+                              rtol relative to the zero-guess residual.  A
+                              given P has its mean removed first: pressure is
+                              defined up to a constant here, and StokesPcCG's
+                              answer (from P = 0) has zero mean             */
   int32_t verbose;
   int32_t cheb_degree;     /* Chebyshev smoothing steps per level             */
   double inner_rtol32;     /* FP32 inner tolerance per refinement step        */
