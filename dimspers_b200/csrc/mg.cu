@@ -521,81 +521,30 @@ __global__ void k_cheb_first_x(const T* __restrict__ b, const T* __restrict__ di
   xn.x = xv.x + dv.x; xn.y = xv.y + dv.y;
   reinterpret_cast<X2*>(x)[n] = xn;
 }
-// r -= Ad; d = c1 d + c2 D^-1 r; x += d  (c1, c2 = coef[0], coef[1]); Ad = 0 for the
-// next apply.  Two nodes per thread with 16-byte accesses: with one node per
-// thread (8-byte accesses) the store of zeros into the accumulator the thread
-// has just read halved the kernel's DRAM throughput on B200 (measured: 195 us
-// against 93 us for the 8.4M-node fine level of 512x4096).
-template <typename T>
-struct Pair4;
-template <>
-struct Pair4<float> {
-  float4 v;
-  __device__ __forceinline__ void load(const float* p, int64_t q) { v = reinterpret_cast<const float4*>(p)[q]; }
-  __device__ __forceinline__ void store(float* p, int64_t q) const { reinterpret_cast<float4*>(p)[q] = v; }
-  __device__ __forceinline__ float& operator[](int i) { return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w; }
-};
-template <>
-struct Pair4<double> {
-  double2 lo, hi;
-  __device__ __forceinline__ void load(const double* p, int64_t q) {
-    lo = reinterpret_cast<const double2*>(p)[2 * q];
-    hi = reinterpret_cast<const double2*>(p)[2 * q + 1];
-  }
-  __device__ __forceinline__ void store(double* p, int64_t q) const {
-    reinterpret_cast<double2*>(p)[2 * q] = lo;
-    reinterpret_cast<double2*>(p)[2 * q + 1] = hi;
-  }
-  __device__ __forceinline__ double& operator[](int i) { return i == 0 ? lo.x : i == 1 ? lo.y : i == 2 ? hi.x : hi.y; }
-};
-
+// r -= Ad; d = c1 d + c2 D^-1 r; x += d  (c1, c2 = coef[0], coef[1]); Ad = 0 for the next apply
 template <typename T>
 __global__ void k_cheb_step(T* __restrict__ Ad, const T* __restrict__ dinv, T* __restrict__ x,
                             T* __restrict__ r, T* __restrict__ d, const double* __restrict__ coef, int64_t nnod) {
   grid_dep_wait();
-  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;   // nodes 2q and 2q + 1
-  if (2 * q >= nnod) return;
-  const T c1 = (T)coef[0], c2 = (T)coef[1];
-  if (2 * q + 1 == nnod) {   // an odd last node (the lattice has 2 nct columns, so not reached)
-    const int64_t n = 2 * q;
-    const T r0 = r[2 * n] - Ad[2 * n], r1 = r[2 * n + 1] - Ad[2 * n + 1];
-    T z0, z1;
-    bj_apply_t<T>(dinv, n, r0, r1, z0, z1);
-    const T d0 = c1 * d[2 * n] + c2 * z0, d1 = c1 * d[2 * n + 1] + c2 * z1;
-    Ad[2 * n] = (T)0; Ad[2 * n + 1] = (T)0;
-    r[2 * n] = r0; r[2 * n + 1] = r1;
-    d[2 * n] = d0; d[2 * n + 1] = d1;
-    x[2 * n] += d0; x[2 * n + 1] += d1;
-    return;
-  }
-  Pair4<T> av, rv, dv, xv;
-  av.load(Ad, q);
-  rv.load(r, q);
-  dv.load(d, q);
-  xv.load(x, q);
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nnod) return;
   typedef typename V2<T>::T X2;
-  const X2* di = reinterpret_cast<const X2*>(dinv) + 3 * q;   // a0 b0 | c0 a1 | b1 c1
-  const X2 q0 = di[0], q1 = di[1], q2 = di[2];
-  T rn[4], dn[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) rn[k] = rv[k] - av[k];
-  const T z0 = q0.x * rn[0] + q0.y * rn[1], z1 = q0.y * rn[0] + q1.x * rn[1];
-  const T z2 = q1.y * rn[2] + q2.x * rn[3], z3 = q2.x * rn[2] + q2.y * rn[3];
-  dn[0] = c1 * dv[0] + c2 * z0;
-  dn[1] = c1 * dv[1] + c2 * z1;
-  dn[2] = c1 * dv[2] + c2 * z2;
-  dn[3] = c1 * dv[3] + c2 * z3;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    av[k] = (T)0;
-    rv[k] = rn[k];
-    dv[k] = dn[k];
-    xv[k] += dn[k];
-  }
-  av.store(Ad, q);
-  rv.store(r, q);
-  dv.store(d, q);
-  xv.store(x, q);
+  const X2 av = reinterpret_cast<const X2*>(Ad)[n];
+  const X2 rv = reinterpret_cast<const X2*>(r)[n];
+  const X2 dv = reinterpret_cast<const X2*>(d)[n];
+  const X2 xv = reinterpret_cast<const X2*>(x)[n];
+  const T c1 = (T)coef[0], c2 = (T)coef[1];
+  X2 rn, dn, xn, zero;
+  rn.x = rv.x - av.x; rn.y = rv.y - av.y;
+  T z0, z1;
+  bj_apply_t<T>(dinv, n, rn.x, rn.y, z0, z1);
+  dn.x = c1 * dv.x + c2 * z0; dn.y = c1 * dv.y + c2 * z1;
+  xn.x = xv.x + dn.x; xn.y = xv.y + dn.y;
+  zero.x = (T)0; zero.y = (T)0;
+  reinterpret_cast<X2*>(Ad)[n] = zero;
+  reinterpret_cast<X2*>(r)[n] = rn;
+  reinterpret_cast<X2*>(d)[n] = dn;
+  reinterpret_cast<X2*>(x)[n] = xn;
 }
 // z = D^-1 r (nodal blocks)
 template <typename T>
@@ -1059,7 +1008,7 @@ static void chebyshev(Ctx& c, MGLevel& L, const T* b, T* x, int mode) {
   }
   for (int k = 1; k < L.degree; ++k) {
     launch_apply_K_acc<T, T>(L.g, level_K<T>(L), d, Ad, c.stream);
-    klaunch(k_cheb_step<T>, tpb((nn + 1) / 2), 256, 0, c.stream, Ad, dinv, x, r, d, L.cheb + 2 * k, nn);
+    klaunch(k_cheb_step<T>, tpb(nn), 256, 0, c.stream, Ad, dinv, x, r, d, L.cheb + 2 * k, nn);
   }
   DP_LAUNCH_CHECK();
 }
