@@ -23,6 +23,8 @@ template <typename Tm, typename Tv>
 void launch_apply_K(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s);       // zeroes y
 template <typename Tm, typename Tv>
 void launch_apply_K_acc(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s);   // y += K x
+template <typename Tm, typename Tv>
+void launch_apply_K_sub(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s);   // y -= K x
 void launch_apply_G(Ctx& c, const double* p, double* y);     // y = G p   (zeroes y)
 void launch_apply_GT(Ctx& c, const double* x, double* p);    // p = G^T x (zeroes p)
 

@@ -279,11 +279,11 @@ __device__ inline void fine_node_weights(int a, int b, int ncrc, int Ac, int Bc,
   }
 }
 
-// xf += P xc (per fine node, gather); also zeroes zb (the fine level's residual
-// buffer, which the next apply accumulates into)
+// xf += P xc (per fine node, gather); also sets rf = bf (the fine level's
+// residual buffer, from which the next apply subtracts A xf)
 template <typename T>
-__global__ void k_prolong_add(const T* __restrict__ xc, T* __restrict__ xf, T* __restrict__ zb, int Af, int Bf,
-                              int ncrc, int Ac, int Bc, int pin) {
+__global__ void k_prolong_add(const T* __restrict__ xc, T* __restrict__ xf, const T* __restrict__ bf,
+                              T* __restrict__ rf, int Af, int Bf, int ncrc, int Ac, int Bc, int pin) {
   grid_dep_wait();
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= Af * Bf) return;
@@ -299,6 +299,7 @@ __global__ void k_prolong_add(const T* __restrict__ xc, T* __restrict__ xf, T* _
 #pragma unroll
   for (int k = 0; k < 6; ++k) v[k] = xc2[cn[k]];
   X2 xv = reinterpret_cast<const X2*>(xf)[n];
+  const X2 bv = reinterpret_cast<const X2*>(bf)[n];
   T s0 = (T)0, s1 = (T)0;
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
@@ -307,20 +308,18 @@ __global__ void k_prolong_add(const T* __restrict__ xc, T* __restrict__ xf, T* _
   }
   if (!dof_fixed(a, b, 0, Af - 1, pin)) xv.x += s0;
   if (!dof_fixed(a, b, 1, Af - 1, pin)) xv.y += s1;
-  X2 zero;
-  zero.x = (T)0;
-  zero.y = (T)0;
   reinterpret_cast<X2*>(xf)[n] = xv;
-  reinterpret_cast<X2*>(zb)[n] = zero;
+  reinterpret_cast<X2*>(rf)[n] = bv;
 }
 
-// bc = P^T (r - t) per coarse node (gather over the class stencil); constrained
-// DOFs of either level are excluded.  blockIdx.y is the parity class, so the
+// bc = P^T (r - t) per coarse node (t = null: P^T r; gather over the class
+// stencil); constrained DOFs of either level are excluded.  blockIdx.y is the parity class, so the
 // stencil reads are uniform across a warp (constant-cache broadcast), and the
 // stencil loop is unrolled with its loads predicated rather than branched, so
 // a thread keeps several gathers in flight.
 // first != 0 also takes the coarse level's first Chebyshev step from x = 0
-// (the work of k_cheb_first): rc = bc, dc = xc = coef[0] D^-1 bc, tc = 0.
+// (the work of k_cheb_first): rc = bc, dc = xc = coef[0] D^-1 bc, and tc = 0
+// when tc is given (the cluster tail's levels accumulate into t).
 template <typename T, int LPN>
 __global__ void __launch_bounds__(256) k_restrict_g(const T* __restrict__ r, const T* __restrict__ t, T* __restrict__ bc,
                                                     int Af, int Bf, int Ac, int Bc, int pin, int first,
@@ -352,7 +351,10 @@ __global__ void __launch_bounds__(256) k_restrict_g(const T* __restrict__ r, con
     b -= (b >= Bf) ? Bf : 0;
     const bool in = a >= 0 && a < Af;
     const int f = in ? a + Af * b : 0;
-    const X2 rv = r2[f], tv = t2[f];
+    const X2 rv = r2[f];
+    X2 tv;
+    if (t2) tv = t2[f];
+    else { tv.x = (T)0; tv.y = (T)0; }
     const double w = c_rtab.w[cls][jj];
     const double w0 = (in && !dof_fixed(a, b, 0, Af - 1, pin)) ? w : 0.0;
     const double w1 = (in && !dof_fixed(a, b, 1, Af - 1, pin)) ? w : 0.0;
@@ -375,7 +377,7 @@ __global__ void __launch_bounds__(256) k_restrict_g(const T* __restrict__ r, con
     const double it = coef_c[0];
     double z0, z1;
     bj_apply<T>(dinv_c, n, b0, b1, z0, z1);
-    tc[2 * n] = (T)0; tc[2 * n + 1] = (T)0;
+    if (tc) { tc[2 * n] = (T)0; tc[2 * n + 1] = (T)0; }
     rc[2 * n] = (T)b0; rc[2 * n + 1] = (T)b1;
     dc[2 * n] = (T)(it * z0); dc[2 * n + 1] = (T)(it * z1);
     xc[2 * n] = (T)(it * z0); xc[2 * n + 1] = (T)(it * z1);
@@ -416,9 +418,14 @@ __global__ void __launch_bounds__(256) k_restrict_tile(const T* __restrict__ r, 
     v.y = (T)0;
     if (a >= 0 && a < Af) {
       const int64_t f = a + (int64_t)Af * b;
-      const X2 rv = r2[f], tv = t2[f];
-      if (!dof_fixed(a, b, 0, Af - 1, pin)) v.x = rv.x - tv.x;
-      if (!dof_fixed(a, b, 1, Af - 1, pin)) v.y = rv.y - tv.y;
+      X2 rv = r2[f];
+      if (t2) {
+        const X2 tv = t2[f];
+        rv.x -= tv.x;
+        rv.y -= tv.y;
+      }
+      if (!dof_fixed(a, b, 0, Af - 1, pin)) v.x = rv.x;
+      if (!dof_fixed(a, b, 1, Af - 1, pin)) v.y = rv.y;
     }
     sp[lb][la] = v;
   }
@@ -450,12 +457,15 @@ __global__ void __launch_bounds__(256) k_restrict_tile(const T* __restrict__ r, 
     const T a = dinv_c[3 * (int64_t)n], bb = dinv_c[3 * (int64_t)n + 1], c = dinv_c[3 * (int64_t)n + 2];
     z0 = a * b0 + bb * b1;
     z1 = bb * b0 + c * b1;
-    X2 zero, dv;
-    zero.x = (T)0;
-    zero.y = (T)0;
+    X2 dv;
     dv.x = it * z0;
     dv.y = it * z1;
-    reinterpret_cast<X2*>(tc)[n] = zero;
+    if (tc) {
+      X2 zero;
+      zero.x = (T)0;
+      zero.y = (T)0;
+      reinterpret_cast<X2*>(tc)[n] = zero;
+    }
     reinterpret_cast<X2*>(rc)[n] = bv;
     reinterpret_cast<X2*>(dc)[n] = dv;
     reinterpret_cast<X2*>(xc)[n] = dv;
@@ -463,8 +473,10 @@ __global__ void __launch_bounds__(256) k_restrict_tile(const T* __restrict__ r, 
 }
 
 // ---- Chebyshev smoother vector steps (per node, coefficients read from device) --
-// first step from x = 0: r = b, d = (1/theta) D^-1 b, x = d
-// (every Chebyshev kernel also zeroes t, which the next apply accumulates into)
+// The residual r lives in one buffer that the applies between the steps update
+// in place (r -= A d, launch_apply_K_sub), so a step reads r, d, x and the
+// block inverse and writes only d and x: no accumulator is zeroed, re-read or
+// subtracted (52 instead of 76 bytes per FP32 node).
 // The three kernels compute in the precision of the level (FP32 on the FP32
 // hierarchy) and move each node's pair of components with one 8/16-byte
 // access, all loads issued before the arithmetic.
@@ -475,10 +487,10 @@ __device__ __forceinline__ void bj_apply_t(const T* __restrict__ dinv, int64_t n
   z1 = b * r0 + c * r1;
 }
 
+// first step from x = 0: r = b, d = (1/theta) D^-1 b, x = d
 template <typename T>
 __global__ void k_cheb_first(const T* __restrict__ b, const T* __restrict__ dinv, T* __restrict__ x,
-                             T* __restrict__ r, T* __restrict__ d, T* __restrict__ t, const double* __restrict__ coef,
-                             int64_t nnod) {
+                             T* __restrict__ r, T* __restrict__ d, const double* __restrict__ coef, int64_t nnod) {
   grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
@@ -487,62 +499,49 @@ __global__ void k_cheb_first(const T* __restrict__ b, const T* __restrict__ dinv
   const T it = (T)coef[0];
   T z0, z1;
   bj_apply_t<T>(dinv, n, bv.x, bv.y, z0, z1);
-  X2 zero, dv;
-  zero.x = (T)0; zero.y = (T)0;
+  X2 dv;
   dv.x = it * z0; dv.y = it * z1;
-  reinterpret_cast<X2*>(t)[n] = zero;
   reinterpret_cast<X2*>(r)[n] = bv;
   reinterpret_cast<X2*>(d)[n] = dv;
   reinterpret_cast<X2*>(x)[n] = dv;
 }
-// first step from a given x: r = b - Ax (Ax in r on entry), d = (1/theta) D^-1 r, x += d
+// first step from a given x (r = b - Ax on entry): d = (1/theta) D^-1 r, x += d
 template <typename T>
-__global__ void k_cheb_first_x(const T* __restrict__ b, const T* __restrict__ dinv, T* __restrict__ x,
-                               T* __restrict__ r, T* __restrict__ d, T* __restrict__ t,
-                               const double* __restrict__ coef, int64_t nnod) {
+__global__ void k_cheb_first_x(const T* __restrict__ r, const T* __restrict__ dinv, T* __restrict__ x,
+                               T* __restrict__ d, const double* __restrict__ coef, int64_t nnod) {
   grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
   typedef typename V2<T>::T X2;
-  const X2 bv = reinterpret_cast<const X2*>(b)[n];
-  const X2 av = reinterpret_cast<const X2*>(r)[n];
+  const X2 rv = reinterpret_cast<const X2*>(r)[n];
   const X2 xv = reinterpret_cast<const X2*>(x)[n];
   const T it = (T)coef[0];
-  X2 rv, dv, zero;
-  rv.x = bv.x - av.x; rv.y = bv.y - av.y;
+  X2 dv;
   T z0, z1;
   bj_apply_t<T>(dinv, n, rv.x, rv.y, z0, z1);
   dv.x = it * z0; dv.y = it * z1;
-  zero.x = (T)0; zero.y = (T)0;
-  reinterpret_cast<X2*>(t)[n] = zero;
-  reinterpret_cast<X2*>(r)[n] = rv;
   reinterpret_cast<X2*>(d)[n] = dv;
   X2 xn;
   xn.x = xv.x + dv.x; xn.y = xv.y + dv.y;
   reinterpret_cast<X2*>(x)[n] = xn;
 }
-// r -= Ad; d = c1 d + c2 D^-1 r; x += d  (c1, c2 = coef[0], coef[1]); Ad = 0 for the next apply
+// d = c1 d + c2 D^-1 r; x += d  (c1, c2 = coef[0], coef[1]; r already holds r - A d_prev)
 template <typename T>
-__global__ void k_cheb_step(T* __restrict__ Ad, const T* __restrict__ dinv, T* __restrict__ x,
-                            T* __restrict__ r, T* __restrict__ d, const double* __restrict__ coef, int64_t nnod) {
+__global__ void k_cheb_step(const T* __restrict__ r, const T* __restrict__ dinv, T* __restrict__ x,
+                            T* __restrict__ d, const double* __restrict__ coef, int64_t nnod) {
   grid_dep_wait();
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnod) return;
   typedef typename V2<T>::T X2;
-  const X2 av = reinterpret_cast<const X2*>(Ad)[n];
   const X2 rv = reinterpret_cast<const X2*>(r)[n];
   const X2 dv = reinterpret_cast<const X2*>(d)[n];
   const X2 xv = reinterpret_cast<const X2*>(x)[n];
   const T c1 = (T)coef[0], c2 = (T)coef[1];
-  X2 rn, dn, xn, zero;
-  rn.x = rv.x - av.x; rn.y = rv.y - av.y;
+  X2 dn, xn;
   T z0, z1;
-  bj_apply_t<T>(dinv, n, rn.x, rn.y, z0, z1);
+  bj_apply_t<T>(dinv, n, rv.x, rv.y, z0, z1);
   dn.x = c1 * dv.x + c2 * z0; dn.y = c1 * dv.y + c2 * z1;
   xn.x = xv.x + dn.x; xn.y = xv.y + dn.y;
-  zero.x = (T)0; zero.y = (T)0;
-  reinterpret_cast<X2*>(Ad)[n] = zero;
-  reinterpret_cast<X2*>(r)[n] = rn;
   reinterpret_cast<X2*>(d)[n] = dn;
   reinterpret_cast<X2*>(x)[n] = xn;
 }
@@ -991,24 +990,24 @@ void mg_setup(Ctx& c, int precision, const MGOptions& o) {
 // Chebyshev smoothing of A x = b on level L.  mode 0: start from x = 0;
 // mode 1: start from x = 0 with the first step already taken (fused into the
 // restriction that produced b); mode 2: start from the given x, with L.r
-// holding zeros on entry (the prolongation zeroes it).  The recurrence
+// holding b on entry (the prolongation copies it there).  The recurrence
 // coefficients live in L.cheb on the device, so this sequence is the same for
 // every assembly and is captured once into the solve graph.
 // On exit r = b - A (x - d_last), i.e. the true residual is r - A d_last.
 template <typename T>
 static void chebyshev(Ctx& c, MGLevel& L, const T* b, T* x, int mode) {
   const int64_t nn = L.g.nnod;
-  T* r = (T*)L.r; T* d = (T*)L.d; T* Ad = (T*)L.t;
+  T* r = (T*)L.r; T* d = (T*)L.d;
   const T* dinv = level_dinv<T>(L);
   if (mode == 0) {
-    klaunch(k_cheb_first<T>, tpb(nn), 256, 0, c.stream, b, dinv, x, r, d, Ad, L.cheb, nn);
+    klaunch(k_cheb_first<T>, tpb(nn), 256, 0, c.stream, b, dinv, x, r, d, L.cheb, nn);
   } else if (mode == 2) {
-    launch_apply_K_acc<T, T>(L.g, level_K<T>(L), x, r, c.stream);
-    klaunch(k_cheb_first_x<T>, tpb(nn), 256, 0, c.stream, b, dinv, x, r, d, Ad, L.cheb, nn);
+    launch_apply_K_sub<T, T>(L.g, level_K<T>(L), x, r, c.stream);
+    klaunch(k_cheb_first_x<T>, tpb(nn), 256, 0, c.stream, (const T*)r, dinv, x, d, L.cheb, nn);
   }
   for (int k = 1; k < L.degree; ++k) {
-    launch_apply_K_acc<T, T>(L.g, level_K<T>(L), d, Ad, c.stream);
-    klaunch(k_cheb_step<T>, tpb(nn), 256, 0, c.stream, Ad, dinv, x, r, d, L.cheb + 2 * k, nn);
+    launch_apply_K_sub<T, T>(L.g, level_K<T>(L), d, r, c.stream);
+    klaunch(k_cheb_step<T>, tpb(nn), 256, 0, c.stream, (const T*)r, dinv, x, d, L.cheb + 2 * k, nn);
   }
   DP_LAUNCH_CHECK();
 }
@@ -1032,7 +1031,7 @@ static void vcycle(Ctx& c, size_t l, const T* b, T* x, const MGOptions& o, bool 
     } else {
       chebyshev<T>(c, L, b, x, first_done ? 1 : 0);
       for (int s = 1; s < o.coarse_sweeps; ++s) {
-        DP_CUDA(cudaMemsetAsync(L.r, 0, sizeof(T) * 2 * L.g.nnod, c.stream));
+        DP_CUDA(cudaMemcpyAsync(L.r, b, sizeof(T) * 2 * L.g.nnod, cudaMemcpyDeviceToDevice, c.stream));
         chebyshev<T>(c, L, b, x, 2);
       }
     }
@@ -1040,32 +1039,34 @@ static void vcycle(Ctx& c, size_t l, const T* b, T* x, const MGOptions& o, bool 
   }
   MGLevel& C = c.mg[l + 1];
   T* r = (T*)L.r;
-  T* t = (T*)L.t;
   T* bc = (T*)C.b;
   T* xc = (T*)C.x;
-  // pre-smoothing, then restrict the true residual r - A d_last (and take the
-  // coarse level's first smoothing step in the same pass unless it is solved densely)
+  // pre-smoothing, r -= A d_last (the true residual), then restrict it (and take
+  // the coarse level's first smoothing step in the same pass unless it is
+  // solved densely)
   chebyshev<T>(c, L, b, x, first_done ? 1 : 0);
-  launch_apply_K_acc<T, T>(L.g, level_K<T>(L), (const T*)L.d, t, c.stream);
+  launch_apply_K_sub<T, T>(L.g, level_K<T>(L), (const T*)L.d, r, c.stream);
   const bool fuse = !(l + 2 == c.mg.size() && dense_coarsest);
+  // the cluster tail's smoother accumulates A d into t, which starts at zero
+  T* tc = (l + 1 == tail_start(c, o)) ? (T*)C.t : nullptr;
   const int nA0 = (int)((C.g.A() + 1) >> 1);  // coarse nodes per parity class (upper bound)
   // the tiled form needs whole tiles along theta (its patch then wraps at most once)
   const bool small = C.g.nnod < 32768 || C.g.B() % kRTile != 0;
   if (small) {
     dim3 grid((unsigned)div_up(4 * (int64_t)nA0 * (C.g.B() >> 1), 256), 4);
-    klaunch(k_restrict_g<T, 4>, grid, 256, 0, c.stream, (const T*)r, (const T*)t, bc, (int)L.g.A(), (int)L.g.B(),
-            (int)C.g.A(), (int)C.g.B(), C.g.pin, fuse ? 1 : 0, (const T*)level_dinv<T>(C), xc, (T*)C.r, (T*)C.d,
-            (T*)C.t, (const double*)C.cheb);
+    klaunch(k_restrict_g<T, 4>, grid, 256, 0, c.stream, (const T*)r, (const T*)nullptr, bc, (int)L.g.A(),
+            (int)L.g.B(), (int)C.g.A(), (int)C.g.B(), C.g.pin, fuse ? 1 : 0, (const T*)level_dinv<T>(C), xc, (T*)C.r,
+            (T*)C.d, tc, (const double*)C.cheb);
   } else {
     dim3 grid((unsigned)div_up(C.g.A(), kRTile), (unsigned)div_up(C.g.B(), kRTile));
-    klaunch(k_restrict_tile<T>, grid, 256, 0, c.stream, (const T*)r, (const T*)t, bc, (int)L.g.A(), (int)L.g.B(),
-            (int)C.g.A(), (int)C.g.B(), C.g.pin, fuse ? 1 : 0, (const T*)level_dinv<T>(C), xc, (T*)C.r, (T*)C.d,
-            (T*)C.t, (const double*)C.cheb);
+    klaunch(k_restrict_tile<T>, grid, 256, 0, c.stream, (const T*)r, (const T*)nullptr, bc, (int)L.g.A(),
+            (int)L.g.B(), (int)C.g.A(), (int)C.g.B(), C.g.pin, fuse ? 1 : 0, (const T*)level_dinv<T>(C), xc,
+            (T*)C.r, (T*)C.d, tc, (const double*)C.cheb);
   }
   DP_LAUNCH_CHECK();
   vcycle<T>(c, l + 1, bc, xc, o, fuse);
-  klaunch(k_prolong_add<T>, tpb(L.g.nnod), 256, 0, c.stream, xc, x, r, (int)L.g.A(), (int)L.g.B(), C.g.ncr, (int)C.g.A(),
-                                                          (int)C.g.B(), L.g.pin);
+  klaunch(k_prolong_add<T>, tpb(L.g.nnod), 256, 0, c.stream, (const T*)xc, x, b, r, (int)L.g.A(), (int)L.g.B(),
+          C.g.ncr, (int)C.g.A(), (int)C.g.B(), L.g.pin);
   DP_LAUNCH_CHECK();
   chebyshev<T>(c, L, b, x, 2);
 }

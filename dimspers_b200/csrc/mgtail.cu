@@ -62,7 +62,10 @@ __device__ __forceinline__ void tail_apply(const TailLevel<T>& L, const T* x, T*
   for (int e = tid; e < L.nel; e += nth) apply_element<T, T, true>(L.K, x, y, e, L.ncr, L.A, L.B);
 }
 
-// k_cheb_first per node: r = b, d = x = coef[0] D^-1 b, t = 0
+// The tail's smoother keeps A d in the accumulator t (zeroed by each step)
+// rather than subtracting it from r in the apply as the separate kernels do:
+// the form is older, and the tail is an option that measured slower anyway.
+// First step per node: r = b, d = x = coef[0] D^-1 b, t = 0
 template <typename T>
 __device__ __forceinline__ void tail_cheb_first(const TailLevel<T>& L, int tid, int nth) {
   const double it = L.cheb[0];
@@ -77,7 +80,7 @@ __device__ __forceinline__ void tail_cheb_first(const TailLevel<T>& L, int tid, 
   }
 }
 
-// k_cheb_first_x per node: r = b - (A x held in r), d = coef[0] D^-1 r, x += d, t = 0
+// First step from a given x, per node: r = b - (A x held in r), d = coef[0] D^-1 r, x += d, t = 0
 template <typename T>
 __device__ __forceinline__ void tail_cheb_first_x(const TailLevel<T>& L, int tid, int nth) {
   const double it = L.cheb[0];
@@ -94,7 +97,7 @@ __device__ __forceinline__ void tail_cheb_first_x(const TailLevel<T>& L, int tid
   }
 }
 
-// k_cheb_step per node: r -= t; d = c1 d + c2 D^-1 r; x += d; t = 0
+// Chebyshev step per node: r -= t; d = c1 d + c2 D^-1 r; x += d; t = 0
 template <typename T>
 __device__ __forceinline__ void tail_cheb_step(const TailLevel<T>& L, const double* coef, int tid, int nth) {
   const double c1 = coef[0], c2 = coef[1];
@@ -186,7 +189,7 @@ __device__ void tail_restrict(const TailLevel<T>& F, const TailLevel<T>& C, int 
   }
 }
 
-// F.x += P C.x and F.r = 0 (k_prolong_add)
+// F.x += P C.x and F.r = 0 (the prolongation of k_prolong_add)
 template <typename T>
 __device__ void tail_prolong(const TailLevel<T>& F, const TailLevel<T>& C, int tid, int nth) {
   const int Af = F.A, pin = F.pin;

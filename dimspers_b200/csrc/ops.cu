@@ -53,9 +53,10 @@ __device__ inline int tile_element(int ncr, int wt) {
   return 32 * m + 2 * ncr * it + lane;
 }
 
-// y += K_e x_e for element e.  kL2: read x with ld.global.cg (L2 only), for
-// callers where other CTAs rewrite x during the same kernel.
-template <typename Tm, typename Tv, bool kL2>
+// y += K_e x_e for element e (kSub: y -= K_e x_e).  kL2: read x with
+// ld.global.cg (L2 only), for callers where other CTAs rewrite x during the
+// same kernel.
+template <typename Tm, typename Tv, bool kL2, bool kSub = false>
 __device__ __forceinline__ void apply_element(const Tm* __restrict__ K, const Tv* x, Tv* y, int e, int ncr, int A,
                                               int B) {
   typedef typename KVec<Tm>::V VT;
@@ -102,16 +103,19 @@ __device__ __forceinline__ void apply_element(const Tm* __restrict__ K, const Tv
     }
   }
 #pragma unroll
-  for (int k = 0; k < 6; ++k) atomic_add2(&y[2 * nd[k]], ye[2 * k], ye[2 * k + 1]);
+  for (int k = 0; k < 6; ++k) {
+    if (kSub) atomic_add2(&y[2 * nd[k]], -ye[2 * k], -ye[2 * k + 1]);
+    else atomic_add2(&y[2 * nd[k]], ye[2 * k], ye[2 * k + 1]);
+  }
 }
 
-template <typename Tm, typename Tv>
+template <typename Tm, typename Tv, bool kSub = false>
 __global__ void __launch_bounds__(256) k_apply_K(const Tm* __restrict__ K, const Tv* __restrict__ x,
                                                  Tv* __restrict__ y, int nel, int ncr, int A, int B, int wt) {
   grid_dep_wait();
   const int e = tile_element(ncr, wt);
   if (e >= nel) return;
-  apply_element<Tm, Tv, false>(K, x, y, e, ncr, A, B);
+  apply_element<Tm, Tv, false, kSub>(K, x, y, e, ncr, A, B);
 }
 
 // ---- matrix-free element-by-element K apply (fine level) -------------------------
@@ -125,7 +129,7 @@ __global__ void __launch_bounds__(256) k_apply_K(const Tm* __restrict__ K, const
 // order of the packed apply), so node gathers and atomics are contiguous; the
 // per-ring table is value-major, so the lanes of a warp (consecutive rings)
 // read it with coalesced loads.
-template <typename T>
+template <typename T, bool kSub = false>
 __global__ void __launch_bounds__(256) k_apply_K_mf(const T* __restrict__ Dw, const T* __restrict__ tab,
                                                     const T* __restrict__ x, T* __restrict__ y, int ncr, int nct,
                                                     int A, int B, int pin) {
@@ -205,7 +209,8 @@ __global__ void __launch_bounds__(256) k_apply_K_mf(const T* __restrict__ Dw, co
     const T c = __ldg(tb + (72 + 2 * k) * nring), s = __ldg(tb + (73 + 2 * k) * nring);
     const T y0 = ft[k] ? (T)0 : c * fx[k] - s * fz[k];
     const T y1 = fr[k] ? (T)0 : s * fx[k] + c * fz[k];
-    atomic_add2(&y[2 * nd[k]], y0, y1);
+    if (kSub) atomic_add2(&y[2 * nd[k]], -y0, -y1);
+    else atomic_add2(&y[2 * nd[k]], y0, y1);
   }
 }
 
@@ -244,22 +249,36 @@ void launch_apply_K(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_
 template void launch_apply_K<double, double>(const Level&, const double*, const double*, double*, cudaStream_t);
 template void launch_apply_K<float, float>(const Level&, const float*, const float*, float*, cudaStream_t);
 
-// y += K x (the caller has zeroed y, typically inside the preceding vector kernel)
-template <typename Tm, typename Tv>
-void launch_apply_K_acc(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
+template <bool kSub, typename Tm, typename Tv>
+static void apply_K_into(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
   if (std::is_same<Tm, Tv>::value && mf_data<Tv>(L) && mf_table<Tv>(L)) {
-    klaunch(k_apply_K_mf<Tv>, (int)div_up(L.nel, 256), 256, 0, s, mf_data<Tv>(L), mf_table<Tv>(L), x, y, L.ncr, L.nct,
-            (int)L.A(), (int)L.B(), L.pin);
+    klaunch(k_apply_K_mf<Tv, kSub>, (int)div_up(L.nel, 256), 256, 0, s, mf_data<Tv>(L), mf_table<Tv>(L), x, y, L.ncr,
+            L.nct, (int)L.A(), (int)L.B(), L.pin);
     DP_LAUNCH_CHECK();
     return;
   }
   int blocks, threads, wt;
   apply_tile(L, blocks, threads, wt);
-  klaunch(k_apply_K<Tm, Tv>, blocks, threads, 0, s, K, x, y, (int)L.nel, L.ncr, (int)L.A(), (int)L.B(), wt);
+  klaunch(k_apply_K<Tm, Tv, kSub>, blocks, threads, 0, s, K, x, y, (int)L.nel, L.ncr, (int)L.A(), (int)L.B(), wt);
   DP_LAUNCH_CHECK();
+}
+
+// y += K x (the caller has zeroed y, typically inside the preceding vector kernel)
+template <typename Tm, typename Tv>
+void launch_apply_K_acc(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
+  apply_K_into<false>(L, K, x, y, s);
 }
 template void launch_apply_K_acc<double, double>(const Level&, const double*, const double*, double*, cudaStream_t);
 template void launch_apply_K_acc<float, float>(const Level&, const float*, const float*, float*, cudaStream_t);
+
+// y -= K x: the smoother keeps its residual in y and lets the apply update it
+// in place (no accumulator to zero and re-read)
+template <typename Tm, typename Tv>
+void launch_apply_K_sub(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
+  apply_K_into<true>(L, K, x, y, s);
+}
+template void launch_apply_K_sub<double, double>(const Level&, const double*, const double*, double*, cudaStream_t);
+template void launch_apply_K_sub<float, float>(const Level&, const float*, const float*, float*, cudaStream_t);
 
 // ---- G / G^T ----------------------------------------------------------------
 __device__ inline void element_nodes_dev(int e, int ncr, int A, int B, int nd[6]) {
