@@ -580,8 +580,9 @@ def solve_bytes_model(nr, nt, outer, inner, pressure="discontinuous", cheb_degre
     V-cycle per inner iteration): every kernel's reads and writes once, from
     the measured iteration counts.  Per-kernel figures (the kernel table):
     FP32 apply 312 B/element + 16 B/node; FP64 apply 624 B/element + 48 B/node;
-    Chebyshev vector step 76 B/node; restriction 16 B/fine node + 40 B/coarse
-    node; prolongation 24 B/fine node; dense coarsest n^2 x 8 B; inner PCG
+    Chebyshev vector steps 52 B/node, first steps 44 B/node (on the coarse
+    levels the first is fused into the restriction); restriction 8 B/fine node
+    + 44 B/coarse node; prolongation 32 B/fine node; dense coarsest n^2 x 8 B; inner PCG
     vector passes 128 B/DOF; outer: G and G^T 288 B/element + vectors, the
     fused Schur update (5 N_P + 2 N_U) x 8 B and its dots; assembly and
     set-up excluded."""
@@ -600,8 +601,9 @@ def solve_bytes_model(nr, nt, outer, inner, pressure="discontinuous", cheb_degre
             break
         cn = levels[i + 1][1]
         vcycle += 2 * cheb_degree * (312.0 * nel + 16.0 * nnod)          # smoothing and residual applies
-        vcycle += 2 * cheb_degree * 76.0 * nnod                          # Chebyshev vector steps
-        vcycle += 16.0 * nnod + 40.0 * cn + 24.0 * nnod                  # restriction, prolongation
+        vcycle += (44.0 if i == 0 else 0.0) * nnod + 44.0 * nnod         # first steps (pre on the top level, post)
+        vcycle += 2 * (cheb_degree - 1) * 52.0 * nnod                    # Chebyshev vector steps
+        vcycle += 8.0 * nnod + 44.0 * cn + 32.0 * nnod                   # restriction, prolongation
     nel, nnod = levels[0]
     n_u = 2 * nnod
     n_p = 3 * nel if pressure == "discontinuous" else (nr + 1) * nt
