@@ -85,6 +85,7 @@ SIGNATURES = {
     "dp_set_material_ti": (C.c_int, [_P, _P, C.c_int64, _P, _P, _P, _P, C.c_double, C.c_int32]),
     "dp_fse_director": (C.c_int, [_P, _P, _P, _P, C.c_int32]),
     "dp_assemble": (C.c_int, [_P, C.c_int32]),
+    "dp_set_deterministic": (C.c_int, [_P, C.c_int32]),
     "dp_get_element_matrices": (C.c_int, [_P, _P, _P, _P, _P]),
     "dp_solve": (C.c_int, [_P, _P, _P, _P, C.POINTER(SolveOpts), C.POINTER(SolveReport), C.c_int32]),
     "dp_apply_K": (C.c_int, [_P, _P, _P, C.c_int32]),

@@ -89,6 +89,7 @@ struct AsmArgs {
   float* K32;          // 78*nel (may be null)
   double* Gp;          // 36*nel
   double* F;           // 2*nnod, accumulated with atomics (zeroed by caller)
+  double* Fe;          // deterministic mode: element RHS, Fe[(2k + c) nel + e] (F then by k_node_gather)
   double* pcsum;       // npres: disc -> 1/rowsum written; cont -> rowsum accumulated
   double* Minv;        // 6*nel: inverse of the element mass block (discontinuous pressure)
   double* mfD;         // 36*nel or null: omega * Q^T D Q per IP, entry-major (matrix-free apply)
@@ -326,8 +327,13 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs p) {
       p.Gp[(size_t)(i * 12 + 2 * k + 1) * p.nel + e] = fixed[k] ? 0.0 : sn[k] * gx + cs[k] * gz;
     }
     const double fx = ACC(kKe + kGe + kMe + 2 * k), fz = ACC(kKe + kGe + kMe + 2 * k + 1);
-    if (!fixt[k]) atomicAdd(&p.F[2 * (size_t)nd[k]], cs[k] * fx - sn[k] * fz);
-    if (!fixed[k]) atomicAdd(&p.F[2 * (size_t)nd[k] + 1], sn[k] * fx + cs[k] * fz);
+    if (p.Fe) {
+      p.Fe[(size_t)(2 * k) * p.nel + e] = fixt[k] ? 0.0 : cs[k] * fx - sn[k] * fz;
+      p.Fe[(size_t)(2 * k + 1) * p.nel + e] = fixed[k] ? 0.0 : sn[k] * fx + cs[k] * fz;
+    } else {
+      if (!fixt[k]) atomicAdd(&p.F[2 * (size_t)nd[k]], cs[k] * fx - sn[k] * fz);
+      if (!fixed[k]) atomicAdd(&p.F[2 * (size_t)nd[k] + 1], sn[k] * fx + cs[k] * fz);
+    }
   }
   // lumped mass rows
   {
@@ -428,6 +434,7 @@ void launch_assemble(Ctx& c, int precision, const CartOut* cart) {
   a.K64 = c.K64;
   a.K32 = precision >= 1 ? c.K32 : nullptr;
   a.Gp = c.Gp; a.F = c.F; a.pcsum = c.pc; a.Minv = c.Minv;
+  a.Fe = static_cast<double*>(L.det);
   a.mfD = c.mfD64;
   if (cart) a.cart = *cart;
   const size_t smem = sizeof(double) * kAcc * kAsmThreads;
@@ -436,12 +443,13 @@ void launch_assemble(Ctx& c, int precision, const CartOut* cart) {
     DP_CUDA(cudaFuncSetAttribute(k_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr_set = true;
   }
-  DP_CUDA(cudaMemsetAsync(c.F, 0, sizeof(double) * 2 * L.nnod, c.stream));
+  if (!a.Fe) DP_CUDA(cudaMemsetAsync(c.F, 0, sizeof(double) * 2 * L.nnod, c.stream));
   if (c.mesh.pressure == 0) DP_CUDA(cudaMemsetAsync(c.pc, 0, sizeof(double) * c.mesh.npres, c.stream));
   const int grid = (int)div_up(L.nel, kAsmThreads);
   ++g_klaunch;
   k_assemble<<<grid, kAsmThreads, smem, c.stream>>>(a);
   DP_LAUNCH_CHECK();
+  if (a.Fe) launch_node_gather<double>(L, a.Fe, c.F, 2, 2, c.stream);
   if (c.mfT64) {
     ++g_klaunch;
     k_mf_table<<<(int)div_up(2 * L.ncr, 64), 64, 0, c.stream>>>(L.ncr, (int)L.A(), c.theta_lat, c.r_lat, c.mfT64);

@@ -29,7 +29,7 @@ Ctx::~Ctx() {
   mg_free(*this);
   cudaFree(theta_lat); cudaFree(r_lat); cudaFree(ref2lat);
   cudaFree(eta); cudaFree(C); cudaFree(rho_lat); cudaFree(rho_ref);
-  cudaFree(mfD64); cudaFree(mfT64); cudaFree(mfD32); cudaFree(mfT32);
+  cudaFree(mfD64); cudaFree(mfT64); cudaFree(mfD32); cudaFree(mfT32); cudaFree(det_buf);
   cudaFree(K64); cudaFree(K32); cudaFree(Gp); cudaFree(F); cudaFree(pc); cudaFree(Minv); cudaFree(Fscale);
   cudaFree(flush);
   cudaFree(stress_buf);
@@ -168,6 +168,7 @@ static void check_solve_cfg(const Ctx& c, const SolveCfg& cfg) {
     throw BadArg("schur_pc = 1 (element-block mass inverse) needs discontinuous pressure");
   if (cfg.use_guess < 0 || cfg.use_guess > 2) throw BadArg("use_guess must be 0, 1 or 2");
   if (cfg.use_guess == 2 && cfg.host_loop) throw BadArg("the learned-guess mode runs in the graph path only");
+  if (c.fine.det && cfg.matrix_free) throw BadArg("matrix_free applies scatter with atomics: not in deterministic mode");
 }
 
 // FP32 copy of the assembled operator (once per assembly) for the FP32 modes.
@@ -622,6 +623,24 @@ int dp_assemble(dp_ctx* h, int32_t precision) {
     c.assembled = precision;
     c.mg_prec = c.mg.empty() ? -1 : c.mg_prec;  // hierarchy values are rebuilt on the next solve
     DP_CUDA(cudaStreamSynchronize(c.stream));
+    return (int)DP_OK;
+  });
+}
+
+int dp_set_deterministic(dp_ctx* h, int32_t on) {
+  if (!h) return DP_BAD_ARG;
+  Ctx& c = h->c;
+  return guarded(&c, [&] {
+    DP_CUDA(cudaSetDevice(c.device));
+    if (on != 0 && on != 1) throw BadArg("on must be 0 or 1");
+    if (on && c.mesh.pressure != 1)
+      throw BadArg("deterministic mode needs discontinuous pressure (the continuous space's G^T and lumped "
+                   "mass still scatter with atomics)");
+    DP_CUDA(cudaStreamSynchronize(c.stream));
+    if (on && !c.det_buf) dalloc(&c.det_buf, (size_t)kDetPerElem * c.fine.nel);
+    c.fine.det = on ? c.det_buf : nullptr;
+    graph_free(c);                          // the captured launches differ between the modes
+    if (on) c.assembled = -1;               // the right-hand side must be assembled again without atomics
     return (int)DP_OK;
   });
 }

@@ -31,6 +31,7 @@ constexpr int kKe = 78;   // packed lower 12x12
 constexpr int kGe = 36;   // 12x3 column-major
 constexpr int kMe = 6;    // packed lower 3x3
 constexpr int kFe = 12;
+constexpr int kDetPerElem = 18;  // deterministic scratch per element: 6 nodes x up to 3 values
 constexpr int kMfTab = 84;  // per ring of the matrix-free apply: 6 IPs x (6 dN/dx, 6 dN/dz), 6 x (cos, sin)
 
 enum MatKind { MAT_NONE = 0, MAT_ISO = 1, MAT_FULL = 2, MAT_TI = 3 };
@@ -51,6 +52,10 @@ struct Level {
   const double* mfT64 = nullptr;
   const float* mfD32 = nullptr;
   const float* mfT32 = nullptr;
+  // Deterministic mode: scratch for per-element results (kDetPerElem values per
+  // element, level precision), summed per node in a fixed order by
+  // k_node_gather instead of scatter-added with atomics.  Null: atomics.
+  void* det = nullptr;
   int64_t A() const { return 2 * (int64_t)ncr + 1; }
   int64_t B() const { return 2 * (int64_t)nct; }
 };
@@ -107,6 +112,7 @@ struct Ctx {
   float* mfD32 = nullptr;       // FP32 copies for the FP32 levels
   float* mfT32 = nullptr;
   bool mf32_stale = true;       // the FP32 copies predate the last assembly
+  double* det_buf = nullptr;    // kDetPerElem*nel: deterministic mode's element results (dp_set_deterministic)
   double* Gp = nullptr;         // 36*nel
   double* F = nullptr;          // 2*nnod
   double* pc = nullptr;         // npres (1/rowsum M)

@@ -575,7 +575,7 @@ static int64_t graph_key(const SolveCfg& cfg, const Ctx& c) {
          ((int64_t)cfg.mg.apply_warps << 24) | ((int64_t)cfg.mg.apply_warps_t << 28) |
          ((int64_t)cfg.launch_overlap << 32) | ((int64_t)tail_start(c, cfg.mg) << 33) |
          ((int64_t)cfg.matrix_free << 37) |
-         ((int64_t)cfg.true_residual << 38);
+         ((int64_t)cfg.true_residual << 38) | ((int64_t)(c.fine.det != nullptr) << 39);
 }
 
 void graph_free(Ctx& c) {

@@ -25,6 +25,10 @@ template <typename Tm, typename Tv>
 void launch_apply_K_acc(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s);   // y += K x
 template <typename Tm, typename Tv>
 void launch_apply_K_sub(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s);   // y -= K x
+// Deterministic mode: per node, y (mode 0: +=, 1: -=, 2: =) the sum over its
+// elements, in a fixed order, of E[(nc k + c) nel + e] (nc = 2; nc = 3 with mode 2)
+template <typename T>
+void launch_node_gather(const Level& L, const T* E, T* y, int nc, int mode, cudaStream_t s);
 void launch_apply_G(Ctx& c, const double* p, double* y);     // y = G p   (zeroes y)
 void launch_apply_GT(Ctx& c, const double* x, double* p);    // p = G^T x (zeroes p)
 

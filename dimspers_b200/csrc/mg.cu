@@ -213,6 +213,21 @@ __global__ void k_diag_blocks(const T* __restrict__ K, double* __restrict__ diag
   }
 }
 
+// Deterministic form: element e's three block entries at its local node k into
+// E[(3k + c) nel + e], summed per node by k_node_gather.
+template <typename T>
+__global__ void k_diag_blocks_elem(const T* __restrict__ K, double* __restrict__ E, int nel) {
+  grid_dep_wait();
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nel) return;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    E[(size_t)(3 * k + 0) * nel + e] = (double)K[kidx<T>(packed_index12(2 * k, 2 * k), e)];
+    E[(size_t)(3 * k + 1) * nel + e] = (double)K[kidx<T>(packed_index12(2 * k + 1, 2 * k), e)];
+    E[(size_t)(3 * k + 2) * nel + e] = (double)K[kidx<T>(packed_index12(2 * k + 1, 2 * k + 1), e)];
+  }
+}
+
 // Inverse of the nodal block (block = 1) or of its diagonal (block = 0);
 // constrained DOFs get zero rows/columns so the smoother never touches them.
 template <typename T>
@@ -574,6 +589,36 @@ __global__ void k_dense_assemble(const T* __restrict__ K, double* __restrict__ D
     }
 }
 
+// Deterministic form: one CTA walks the elements in order, its threads taking
+// the 78 packed entries of one element at a time.  The entries of one element
+// land on distinct matrix positions (its 12 DOFs are distinct), so the threads
+// never collide, and every position receives its contributions in element
+// order.  The coarsest level has a few hundred elements.
+template <typename T>
+__global__ void __launch_bounds__(128) k_dense_assemble_seq(const T* __restrict__ K, double* __restrict__ D, int nel,
+                                                            int ncr, int A, int B, int n) {
+  grid_dep_wait();
+  const int i = threadIdx.x;
+  int R = 0, C = 0;
+  if (i < kKe) {   // packed entry i -> (R, C), R >= C, column-major lower triangle
+    int c0 = 0, rem = i;
+    while (rem >= 12 - c0) { rem -= 12 - c0; ++c0; }
+    C = c0;
+    R = c0 + rem;
+  }
+  for (int e = 0; e < nel; ++e) {
+    if (i < kKe) {
+      int nd[6];
+      element_nodes_mg(e, ncr, A, B, nd);
+      const double v = (double)K[kidx<T>(packed_index12(R, C), e)];
+      const int gr = 2 * nd[R >> 1] + (R & 1), gc = 2 * nd[C >> 1] + (C & 1);
+      D[(size_t)gr * n + gc] += v;
+      if (R != C) D[(size_t)gc * n + gr] += v;
+    }
+    __syncthreads();
+  }
+}
+
 // Identity on the diagonal of fixed (all-zero) rows, so the matrix stays SPD.
 __global__ void k_dense_fix_diag(double* __restrict__ D, int n) {
   grid_dep_wait();
@@ -896,6 +941,7 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
   for (MGLevel& L : c.mg) {
     L.g.warps = o.apply_warps;
     L.g.warps_t = o.apply_warps_t;
+    L.g.det = c.fine.det;   // one scratch (sized for the fine level) serves every level in turn
     L.g.mfD64 = L.g.mfT64 = nullptr;
     L.g.mfD32 = L.g.mfT32 = nullptr;
   }
@@ -922,9 +968,16 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
   for (size_t l = 0; l < c.mg.size(); ++l) {
     MGLevel& L = c.mg[l];
     L.degree = l == 0 ? deg : deg_coarse;
-    DP_CUDA(cudaMemsetAsync(diag, 0, sizeof(double) * 3 * L.g.nnod, c.stream));
-    klaunch(k_diag_blocks<T>, (int)div_up(L.g.nel, 128), 128, 0, c.stream, level_K<T>(L), diag, (int)L.g.nel, L.g.ncr,
-                                                                       (int)L.g.A(), (int)L.g.B());
+    if (L.g.det) {
+      double* E = static_cast<double*>(L.g.det);
+      klaunch(k_diag_blocks_elem<T>, (int)div_up(L.g.nel, 128), 128, 0, c.stream, level_K<T>(L), E, (int)L.g.nel);
+      DP_LAUNCH_CHECK();
+      launch_node_gather<double>(L.g, E, diag, 3, 2, c.stream);
+    } else {
+      DP_CUDA(cudaMemsetAsync(diag, 0, sizeof(double) * 3 * L.g.nnod, c.stream));
+      klaunch(k_diag_blocks<T>, (int)div_up(L.g.nel, 128), 128, 0, c.stream, level_K<T>(L), diag, (int)L.g.nel,
+              L.g.ncr, (int)L.g.A(), (int)L.g.B());
+    }
     klaunch(k_block_invert<T>, tpb(L.g.nnod), 256, 0, c.stream, diag, level_dinv<T>(L), L.g.nnod, (int)L.g.A(), L.g.pin,
                                                             o.block_jacobi);
     DP_LAUNCH_CHECK();
@@ -956,8 +1009,12 @@ static void mg_setup_t(Ctx& c, const MGOptions& o) {
     double* D = c.coarse_inv;
     double* Inv = D + (size_t)n * n;
     DP_CUDA(cudaMemsetAsync(D, 0, sizeof(double) * n * n, c.stream));
-    klaunch(k_dense_assemble<T>, (int)div_up(L.g.nel, 128), 128, 0, c.stream, level_K<T>(L), D, (int)L.g.nel, L.g.ncr,
-                                                                          (int)L.g.A(), (int)L.g.B(), n);
+    if (L.g.det)
+      klaunch(k_dense_assemble_seq<T>, 1, 128, 0, c.stream, level_K<T>(L), D, (int)L.g.nel, L.g.ncr, (int)L.g.A(),
+              (int)L.g.B(), n);
+    else
+      klaunch(k_dense_assemble<T>, (int)div_up(L.g.nel, 128), 128, 0, c.stream, level_K<T>(L), D, (int)L.g.nel,
+              L.g.ncr, (int)L.g.A(), (int)L.g.B(), n);
     klaunch(k_dense_fix_diag, (int)div_up(n, 256), 256, 0, c.stream, D, n);
     double* buf[2] = {D, Inv};
     double* W = nullptr;   // panel inverse (kGJPanel^2) and T (n x kGJPanel)

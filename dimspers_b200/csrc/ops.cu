@@ -9,6 +9,8 @@
 // Dots: deterministic two-level reduction (warp shuffles -> block -> fixed-order
 // sum of the per-block partials by the last block), the role of mydot /
 // mynorm / vmean in Algebra.jl:104-113 and IterativeSolvers.jl:179-186.
+#include <stdexcept>
+
 #include "kernels.cuh"
 #include "reduce.cuh"
 
@@ -53,12 +55,12 @@ __device__ inline int tile_element(int ncr, int wt) {
   return 32 * m + 2 * ncr * it + lane;
 }
 
-// y += K_e x_e for element e (kSub: y -= K_e x_e).  kL2: read x with
-// ld.global.cg (L2 only), for callers where other CTAs rewrite x during the
-// same kernel.
-template <typename Tm, typename Tv, bool kL2, bool kSub = false>
-__device__ __forceinline__ void apply_element(const Tm* __restrict__ K, const Tv* x, Tv* y, int e, int ncr, int A,
-                                              int B) {
+// ye = K_e x_e for element e, with the lattice index of each of its 6 nodes.
+// kL2: read x with ld.global.cg (L2 only), for callers where other CTAs
+// rewrite x during the same kernel.
+template <typename Tm, typename Tv, bool kL2>
+__device__ __forceinline__ void element_product(const Tm* __restrict__ K, const Tv* x, int e, int ncr, int A, int B,
+                                                int nd[6], Tv ye[12]) {
   typedef typename KVec<Tm>::V VT;
   constexpr int NV = KVec<Tm>::n;
   constexpr int PER = sizeof(VT) / sizeof(Tm);
@@ -69,7 +71,6 @@ __device__ __forceinline__ void apply_element(const Tm* __restrict__ K, const Tv
   const int q = e >> 1, t = e & 1;
   const int ir = q % ncr, it = q / ncr;
   const int a0 = 2 * ir, b0 = 2 * it;
-  int nd[6];
   {
     int bb[6], aa[6];
     if (t == 0) {
@@ -84,7 +85,7 @@ __device__ __forceinline__ void apply_element(const Tm* __restrict__ K, const Tv
   }
   typedef typename V2<Tv>::T X2;
   const X2* x2 = reinterpret_cast<const X2*>(x);
-  Tv xe[12], ye[12];
+  Tv xe[12];
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
     const X2 v = kL2 ? __ldcg(x2 + nd[k]) : x2[nd[k]];
@@ -102,6 +103,15 @@ __device__ __forceinline__ void apply_element(const Tm* __restrict__ K, const Tv
       if (R != C) ye[C] += kv * xe[R];
     }
   }
+}
+
+// y += K_e x_e for element e (kSub: y -= K_e x_e), scatter-added with atomics.
+template <typename Tm, typename Tv, bool kL2, bool kSub = false>
+__device__ __forceinline__ void apply_element(const Tm* __restrict__ K, const Tv* x, Tv* y, int e, int ncr, int A,
+                                              int B) {
+  int nd[6];
+  Tv ye[12];
+  element_product<Tm, Tv, kL2>(K, x, e, ncr, A, B, nd, ye);
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
     if (kSub) atomic_add2(&y[2 * nd[k]], -ye[2 * k], -ye[2 * k + 1]);
@@ -117,6 +127,88 @@ __global__ void __launch_bounds__(256) k_apply_K(const Tm* __restrict__ K, const
   if (e >= nel) return;
   apply_element<Tm, Tv, false, kSub>(K, x, y, e, ncr, A, B);
 }
+
+// Deterministic form, pass 1: E[(2k + c) nel + e] = (K_e x_e) of local node k,
+// component c (no atomics; k_node_gather sums the nodes in a fixed order).
+template <typename Tm, typename Tv>
+__global__ void __launch_bounds__(256) k_apply_K_elem(const Tm* __restrict__ K, const Tv* __restrict__ x,
+                                                      Tv* __restrict__ E, int nel, int ncr, int A, int B) {
+  grid_dep_wait();
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nel) return;
+  int nd[6];
+  Tv ye[12];
+  element_product<Tm, Tv, false>(K, x, e, ncr, A, B, nd, ye);
+#pragma unroll
+  for (int d = 0; d < 12; ++d) E[(int64_t)d * nel + e] = ye[d];
+}
+
+// Local node k of triangle type t sits at lattice offset (kLocA, kLocB) from
+// its cell origin (2 ir, 2 it): the node order of element_product.
+__host__ __device__ constexpr int loc_a(int t, int k) {
+  return t == 0 ? (k == 2 ? 2 : (k >= 4 ? 1 : 0)) : (k == 0 ? 0 : (k == 3 || k == 5 ? 1 : 2));
+}
+__host__ __device__ constexpr int loc_b(int t, int k) {
+  return t == 0 ? (k == 1 ? 2 : (k == 3 || k == 4 ? 1 : 0)) : (k == 2 ? 0 : (k >= 4 ? 1 : 2));
+}
+
+// Deterministic form, pass 2: per lattice node n, the sum of E over the
+// elements that contain it, taken in a fixed order (triangle type t = 0, 1,
+// then local node k = 0..5), so the result is the same bit for bit in every
+// run.  E[(NC k + c) nel + e] holds element e's value c at its local node k.
+// MODE 0: y[NC n + c] += s; 1: y -= s; 2: y = s.
+template <typename T, int NC, int MODE>
+__global__ void __launch_bounds__(256) k_node_gather(const T* __restrict__ E, T* __restrict__ y, int ncr, int nct,
+                                                     int64_t nel) {
+  grid_dep_wait();
+  const int A = 2 * ncr + 1, B = 2 * nct;
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= (int64_t)A * B) return;
+  const int b = (int)(n / A), a = (int)(n - (int64_t)b * A);
+  T s[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) s[c] = (T)0;
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const int da = a - loc_a(t, k);
+      int db = b - loc_b(t, k);
+      if (da < 0 || (da & 1) || (da >> 1) >= ncr || (db & 1)) continue;
+      if (db < 0) db += B;
+      const int64_t e = 2 * ((int64_t)(da >> 1) + (int64_t)ncr * (db >> 1)) + t;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) s[c] += E[(int64_t)(NC * k + c) * nel + e];
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    T* p = y + NC * n + c;
+    if (MODE == 0) *p += s[c];
+    else if (MODE == 1) *p -= s[c];
+    else *p = s[c];
+  }
+}
+
+template <typename T>
+void launch_node_gather(const Level& L, const T* E, T* y, int nc, int mode, cudaStream_t s) {
+  const int grid = (int)div_up(L.nnod, 256);
+#define DP_GATHER(NC, M) \
+  klaunch(k_node_gather<T, NC, M>, grid, 256, 0, s, E, y, L.ncr, L.nct, (int64_t)L.nel)
+  if (nc == 2) {
+    if (mode == 0) DP_GATHER(2, 0);
+    else if (mode == 1) DP_GATHER(2, 1);
+    else DP_GATHER(2, 2);
+  } else if (nc == 3 && mode == 2) {
+    DP_GATHER(3, 2);
+  } else {
+    throw std::runtime_error("launch_node_gather: unsupported layout");
+  }
+#undef DP_GATHER
+  DP_LAUNCH_CHECK();
+}
+template void launch_node_gather<double>(const Level&, const double*, double*, int, int, cudaStream_t);
+template void launch_node_gather<float>(const Level&, const float*, float*, int, int, cudaStream_t);
 
 // ---- matrix-free element-by-element K apply (fine level) -------------------------
 // K_e (polar DOFs, constrained rows/columns masked) = sum_ip B0^T Dw_ip B0, with
@@ -241,16 +333,21 @@ static void apply_tile(const Level& L, int& blocks, int& threads, int& wt) {
   }
 }
 
-template <typename Tm, typename Tv>
-void launch_apply_K(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
-  DP_CUDA(cudaMemsetAsync(y, 0, sizeof(Tv) * 2 * L.nnod, s));
-  launch_apply_K_acc<Tm, Tv>(L, K, x, y, s);
-}
-template void launch_apply_K<double, double>(const Level&, const double*, const double*, double*, cudaStream_t);
-template void launch_apply_K<float, float>(const Level&, const float*, const float*, float*, cudaStream_t);
-
-template <bool kSub, typename Tm, typename Tv>
+// kMode 0: y += K x, 1: y -= K x, 2: y = K x (the atomic form zeroes y
+// first).  With L.det set the apply runs as two passes without atomics
+// (element results, then the fixed-order node gather).
+template <int kMode, typename Tm, typename Tv>
 static void apply_K_into(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
+  constexpr bool kSub = kMode == 1;
+  if (L.det) {
+    Tv* E = static_cast<Tv*>(L.det);
+    klaunch(k_apply_K_elem<Tm, Tv>, (int)div_up(L.nel, 256), 256, 0, s, K, x, E, (int)L.nel, L.ncr, (int)L.A(),
+            (int)L.B());
+    DP_LAUNCH_CHECK();
+    launch_node_gather<Tv>(L, E, y, 2, kMode, s);
+    return;
+  }
+  if (kMode == 2) DP_CUDA(cudaMemsetAsync(y, 0, sizeof(Tv) * 2 * L.nnod, s));
   if (std::is_same<Tm, Tv>::value && mf_data<Tv>(L) && mf_table<Tv>(L)) {
     klaunch(k_apply_K_mf<Tv, kSub>, (int)div_up(L.nel, 256), 256, 0, s, mf_data<Tv>(L), mf_table<Tv>(L), x, y, L.ncr,
             L.nct, (int)L.A(), (int)L.B(), L.pin);
@@ -263,10 +360,17 @@ static void apply_K_into(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaSt
   DP_LAUNCH_CHECK();
 }
 
+template <typename Tm, typename Tv>
+void launch_apply_K(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
+  apply_K_into<2>(L, K, x, y, s);
+}
+template void launch_apply_K<double, double>(const Level&, const double*, const double*, double*, cudaStream_t);
+template void launch_apply_K<float, float>(const Level&, const float*, const float*, float*, cudaStream_t);
+
 // y += K x (the caller has zeroed y, typically inside the preceding vector kernel)
 template <typename Tm, typename Tv>
 void launch_apply_K_acc(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
-  apply_K_into<false>(L, K, x, y, s);
+  apply_K_into<0>(L, K, x, y, s);
 }
 template void launch_apply_K_acc<double, double>(const Level&, const double*, const double*, double*, cudaStream_t);
 template void launch_apply_K_acc<float, float>(const Level&, const float*, const float*, float*, cudaStream_t);
@@ -275,7 +379,7 @@ template void launch_apply_K_acc<float, float>(const Level&, const float*, const
 // in place (no accumulator to zero and re-read)
 template <typename Tm, typename Tv>
 void launch_apply_K_sub(const Level& L, const Tm* K, const Tv* x, Tv* y, cudaStream_t s) {
-  apply_K_into<true>(L, K, x, y, s);
+  apply_K_into<1>(L, K, x, y, s);
 }
 template void launch_apply_K_sub<double, double>(const Level&, const double*, const double*, double*, cudaStream_t);
 template void launch_apply_K_sub<float, float>(const Level&, const float*, const float*, float*, cudaStream_t);
@@ -326,6 +430,22 @@ __global__ void k_apply_G(const double* __restrict__ G, const double* __restrict
                      G[(size_t)(24 + d) * nel + e] * p2;
     atomicAdd(&y[2 * nd[d >> 1] + (d & 1)], v);
   }
+}
+
+// Deterministic form of the G apply, pass 1: element e's 12 values of G_e p_e
+// into E[d nel + e] (k_node_gather sums them per node).
+__global__ void k_apply_G_elem(const double* __restrict__ G, const double* __restrict__ p, double* __restrict__ E,
+                               int nel, int ncr, int nct, int pressure) {
+  grid_dep_wait();
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nel) return;
+  int pd[3];
+  element_pdofs_dev(e, ncr, nct, pressure, pd);
+  const double p0 = p[pd[0]], p1 = p[pd[1]], p2 = p[pd[2]];
+#pragma unroll
+  for (int d = 0; d < 12; ++d)
+    E[(size_t)d * nel + e] = G[(size_t)d * nel + e] * p0 + G[(size_t)(12 + d) * nel + e] * p1 +
+                             G[(size_t)(24 + d) * nel + e] * p2;
 }
 
 __global__ void k_apply_GT(const double* __restrict__ G, const double* __restrict__ x, double* __restrict__ p,
@@ -403,6 +523,14 @@ __global__ void __launch_bounds__(128) k_apply_G_warp(const double* __restrict__
 
 void launch_apply_G(Ctx& c, const double* p, double* y) {
   const Level& L = c.fine;
+  if (L.det) {
+    double* E = static_cast<double*>(L.det);
+    klaunch(k_apply_G_elem, (int)div_up(L.nel, 128), 128, 0, c.stream, c.Gp, p, E, (int)L.nel, L.ncr, L.nct,
+            c.mesh.pressure);
+    DP_LAUNCH_CHECK();
+    launch_node_gather<double>(L, E, y, 2, 2, c.stream);
+    return;
+  }
   DP_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * 2 * L.nnod, c.stream));
   if (L.ncr % 16 == 0) {
     // nel = 2 ncr nct is then a multiple of 32 and every warp is whole

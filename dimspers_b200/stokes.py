@@ -186,6 +186,11 @@ class StokesContext:
     def assemble(self, precision=0):
         self._chk(lib().dp_assemble(self.h, int(precision)))
 
+    def set_deterministic(self, on=True):
+        """Scatter without atomics (fixed-order per-node sums), so repeated
+        solves are bit-identical; discards the assembly when switched on."""
+        self._chk(lib().dp_set_deterministic(self.h, 1 if on else 0))
+
     def element_matrices(self):
         Ke = np.empty((self.nel, 78))
         Ge = np.empty((self.nel, 36))

@@ -205,6 +205,18 @@ int dp_fse_director(dp_ctx* ctx, const double* F, double* dir_x, double* dir_y, 
 /* Element assembly + rotation + BC mask on the device (precision: dp_precision). */
 int dp_assemble(dp_ctx* ctx, int32_t precision);
 
+/* Deterministic mode (on = 1): every scatter of the solve path (the K and G
+ * applies in FP32 and FP64, the right-hand side, the multigrid diagonal blocks
+ * and the dense coarsest matrix) runs without atomics, as element results
+ * summed per node in a fixed order, so repeated solves of the same inputs give
+ * the same U, P and iteration counts bit for bit.  Costs 144 bytes of device
+ * scratch per element and two passes per apply.  Needs discontinuous
+ * pressure and matrix_free = 0.  Switching it on discards the current assembly
+ * (call dp_assemble again); on = 0 returns to the atomic scatter.  (The
+ * reference's threaded assembly gets race freedom from element colouring,
+ * coloring.jl:1-64; the atomic device scatter has none of its ordering.) */
+int dp_set_deterministic(dp_ctx* ctx, int32_t on);
+
 /* Copy the un-rotated Cartesian element blocks in the reference layouts
  * (K_all 78 x nel, G_all 36 x nel, M_all 6 x nel, Fb_all 12 x nel, column-major).
  * Any pointer may be NULL. */
