@@ -24,6 +24,9 @@ device):
            iterations: Galerkin levels, Gauss-Jordan coarse inverse, the
            FP64 Krylov kernels, G and G^T, the compensated Schur kernels
   solve64  the same in FP64 with the lumped Schur preconditioner
+  det      solve32 in deterministic mode: the element-result kernels of the
+           applies, right-hand side and diagonal blocks, the per-node gathers,
+           the sequential dense coarse assembly
   inner    the graph solve's inner-iteration vector kernels (launched outside
            the graph: ncu cannot look inside conditional graph nodes)
   post     stress post-processor, viscosity update, FSE, DEM tensor lookup,
@@ -54,9 +57,11 @@ def _stokes(precision):
     return ctx, arm
 
 
-def solve(precision):
+def solve(precision, deterministic=False):
     import torch
     ctx, arm = _stokes(precision)
+    if deterministic:
+        ctx.set_deterministic(True)
     torch.cuda.synchronize()
     with _range("target"):
         ctx.assemble(arm["precision"])
@@ -151,7 +156,7 @@ def cnn():
 
 
 CASES = {"apply32": lambda: apply(0), "apply64": lambda: apply(1), "vcycle": vcycle, "solve32": lambda: solve(1),
-         "solve64": lambda: solve(0), "inner": inner, "post": post, "cnn": cnn}
+         "solve64": lambda: solve(0), "det": lambda: solve(1, True), "inner": inner, "post": post, "cnn": cnn}
 
 if __name__ == "__main__":
     import argparse
