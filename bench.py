@@ -583,7 +583,7 @@ def solve_bytes_model(nr, nt, outer, inner, pressure="discontinuous", cheb_degre
     Chebyshev vector steps 52 B/node, first steps 44 B/node (on the coarse
     levels the first is fused into the restriction); restriction 8 B/fine node
     + 44 B/coarse node; prolongation 32 B/fine node; dense coarsest n^2 x 8 B; inner PCG
-    vector passes 128 B/DOF; outer: G and G^T 288 B/element + vectors, the
+    vector passes 108 B/DOF; outer: G and G^T 288 B/element + vectors, the
     fused Schur update (5 N_P + 2 N_U) x 8 B and its dots; assembly and
     set-up excluded."""
     levels = []
@@ -607,7 +607,7 @@ def solve_bytes_model(nr, nt, outer, inner, pressure="discontinuous", cheb_degre
     nel, nnod = levels[0]
     n_u = 2 * nnod
     n_p = 3 * nel if pressure == "discontinuous" else (nr + 1) * nt
-    per_inner = vcycle + 624.0 * nel + 48.0 * nnod + 128.0 * n_u
+    per_inner = vcycle + 624.0 * nel + 48.0 * nnod + 108.0 * n_u
     per_outer = 2 * (288.0 * nel + 16.0 * nnod + 8.0 * n_p) + (5 * n_p + 2 * n_u) * 8.0 + 4 * 16.0 * n_p
     return inner * per_inner + outer * per_outer
 

@@ -204,7 +204,21 @@ __global__ void k_pcg_dir_g(T* __restrict__ p, const T* __restrict__ z, T* __res
   }
 }
 
-// FP64 residual -> FP32 hierarchy input, scaled by 1/||r|| (keeps FP32 in range)
+// p = s z32 + beta p (s = ||b||, the FP32 V-cycle ran on r / ||b||), Ap = 0:
+// the mixed-precision form reads the FP32 preconditioned residual directly
+__global__ void k_pcg_dir_f32z(double* __restrict__ p, const float* __restrict__ z32, double* __restrict__ Ap,
+                               int64_t n, const double* scal, int yy, int rzn, int rz, const int* it) {
+  grid_dep_wait();
+  const double beta = (*it == 0 || scal[rz] == 0.0) ? 0.0 : scal[rzn] / scal[rz];
+  const double s = sqrt(scal[yy]);
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) {
+    p[i] = s * (double)z32[i] + beta * p[i];
+    Ap[i] = 0.0;  // the next apply accumulates into Ap
+  }
+}
+
+// FP64 residual -> FP32 hierarchy input, scaled by 1/sqrt(scal[irr]) (keeps FP32 in range)
 __global__ void k_r_to_f32(const double* __restrict__ r, float* __restrict__ r32, const double* scal, int irr, int64_t n) {
   grid_dep_wait();
   const double s = 1.0 / sqrt(scal[irr]);
@@ -225,19 +239,16 @@ __global__ void k_bj_mixed(const Td* __restrict__ dinv, const Tv* __restrict__ r
 
 // x += alpha p; r -= alpha Ap; alpha = rzn/pAp; ||r||^2 -> irr
 
-// z = ||r|| z32 (the V-cycle ran on r / ||r||) fused with rz = r . z
-__global__ void __launch_bounds__(kRedThreads) k_z_from_f32_dot(const float* __restrict__ z32, double* __restrict__ z,
-                                                                 const double* __restrict__ r, double* scal, int irr,
-                                                                 int rzn, int64_t n, double* partial,
-                                                                 unsigned int* counter) {
+// rz = r . z with z = ||b|| z32 (the V-cycle ran on r / ||b||); z itself is
+// never stored: k_pcg_dir_f32z reads z32 again
+__global__ void __launch_bounds__(kRedThreads) k_rz_f32(const float* __restrict__ z32, const double* __restrict__ r,
+                                                        double* scal, int yy, int rzn, int64_t n, double* partial,
+                                                        unsigned int* counter) {
   grid_dep_wait();
-  const double sc = sqrt(scal[irr]);
+  const double sc = sqrt(scal[yy]);
   double s = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
-    const double zi = sc * (double)z32[i];
-    z[i] = zi;
-    s += r[i] * zi;
-  }
+  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads)
+    s += r[i] * (sc * (double)z32[i]);
   double v[1] = {s};
   double* o[1] = {scal + rzn};
   grid_finish<1>(v, partial, counter, o);
@@ -245,14 +256,17 @@ __global__ void __launch_bounds__(kRedThreads) k_z_from_f32_dot(const float* __r
 
 // x += alpha p; r -= alpha Ap; ||r||^2 (alpha = rz / pAp from the table); the
 // last block also takes the loop's stopping decision: continue while
-// ||r||^2 > tol^2 ||b||^2 and it < inner_itmax.
+// ||r||^2 > tol^2 ||b||^2 and it < inner_itmax.  r32 != null (FP64 Krylov on
+// the FP32 hierarchy): also writes the next V-cycle's input r / ||b||.
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_pcg_upd_check(T* __restrict__ x, T* __restrict__ r,
                                                                 const T* __restrict__ p, const T* __restrict__ Ap,
                                                                 int64_t n, double* scal, int rz, int rzn, int pap,
                                                                 int irr, double* partial, unsigned int* counter,
-                                                                cudaGraphConditionalHandle h, DevCtl* ctl, int fp32) {
+                                                                cudaGraphConditionalHandle h, DevCtl* ctl, int fp32,
+                                                                float* __restrict__ r32, int yy) {
   grid_dep_wait();
+  const double inv_s = r32 ? 1.0 / sqrt(scal[yy]) : 0.0;
   // a non-positive or non-finite p.Ap (breakdown, e.g. an FP32 operator that
   // rounding made indefinite) leaves x and r unchanged and ends the loop
   const double pap_v = scal[pap];
@@ -263,6 +277,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_upd_check(T* __restrict__ x
     x[i] += (T)(alpha * (double)p[i]);
     const double ri = (double)r[i] - alpha * (double)Ap[i];
     r[i] = (T)ri;
+    if (r32) r32[i] = (float)(inv_s * ri);
     s += ri * ri;
   }
   double v[1] = {s};
@@ -369,20 +384,23 @@ static void emit_pcg(Ctx& c, const SolveCfg& cfg, const T* Kmat, const T* b, T* 
   DP_CUDA(cudaMemcpyAsync(r, b, sizeof(T) * n, cudaMemcpyDeviceToDevice, c.stream));
   if (f32) launch_dot_f(c, (const float*)b, (const float*)b, n, YY);
   else launch_dot(c, (const double*)b, (const double*)b, n, YY);
+  // FP64 Krylov on the FP32 hierarchy: the V-cycle runs on r / ||b|| in FP32
+  // (r32, written by the update kernel of the previous iteration) and its
+  // output z32 is read directly by the dot and the direction update
+  const bool mixed = cfg.inner_pc == 0 && !f32 && c.mg_prec == 1;
+  float* r32 = (float*)c.work[W_F_R];
+  float* z32 = (float*)c.work[W_F_Z];
+  if (mixed) klaunch(k_r_to_f32, g_nb(n), 256, 0, c.stream, (const double*)b, r32, c.scal, YY, n);
   cudaGraphConditionalHandle h = new_handle(c.stream);
   klaunch(k_in_init, 1, 1, 0, c.stream, h, ctl, c.scal, YY, IRR, c.scal, f32 ? 1 : 0, relax);
   DP_LAUNCH_CHECK();
   cudaGraph_t body = add_while(c.stream, h);
   const int* itp = f32 ? &ctl->in32_it : &ctl->in_it;
   capture_body(c, body, depth, f32 ? B_PCG32 : B_PCG64, [&] {
-    const bool mixed = !f32 && c.mg_prec == 1;  // FP64 Krylov, FP32 hierarchy
     if (cfg.inner_pc == 0) {
       if (f32) {
         mg_apply_f(c, (const float*)r, (float*)z, cfg.mg);
       } else if (mixed) {
-        float* r32 = (float*)c.work[W_F_R];
-        float* z32 = (float*)c.work[W_F_Z];
-        klaunch(k_r_to_f32, g_nb(n), 256, 0, c.stream, (const double*)r, r32, c.scal, IRR, n);
         mg_apply_f(c, r32, z32, cfg.mg);
       } else {
         mg_apply(c, (const double*)r, (double*)z, cfg.mg);
@@ -391,17 +409,21 @@ static void emit_pcg(Ctx& c, const SolveCfg& cfg, const T* Kmat, const T* b, T* 
       if (c.mg_prec == 1) klaunch(k_bj_mixed<float, T>, g_nb(L.nnod), 256, 0, c.stream, c.mg[0].dinv32, r, z, L.nnod);
       else klaunch(k_bj_mixed<double, T>, g_nb(L.nnod), 256, 0, c.stream, c.mg[0].dinv64, r, z, L.nnod);
     }
-    if (cfg.inner_pc == 0 && !f32 && c.mg_prec == 1)
-      klaunch(k_z_from_f32_dot, red_grid(n), kRedThreads, 0, c.stream, (const float*)c.work[W_F_Z], (double*)z,
-              (const double*)r, c.scal, IRR, RZN, n, c.partial, c.counter);
+    if (mixed)
+      klaunch(k_rz_f32, red_grid(n), kRedThreads, 0, c.stream, (const float*)z32, (const double*)r, c.scal, YY, RZN, n,
+              c.partial, c.counter);
     else if (f32) launch_dot_f(c, (const float*)r, (const float*)z, n, RZN);
     else launch_dot(c, (const double*)r, (const double*)z, n, RZN);
-    klaunch(k_pcg_dir_g<T>, g_nb(n), 256, 0, c.stream, p, z, Ap, n, c.scal, RZN, RZ, itp);
+    if (mixed)
+      klaunch(k_pcg_dir_f32z, g_nb(n), 256, 0, c.stream, (double*)p, (const float*)z32, (double*)Ap, n,
+              (const double*)c.scal, YY, RZN, RZ, itp);
+    else
+      klaunch(k_pcg_dir_g<T>, g_nb(n), 256, 0, c.stream, p, z, Ap, n, c.scal, RZN, RZ, itp);
     launch_apply_K_acc<T, T>(L, Kmat, p, Ap, c.stream);
     if (f32) launch_dot_f(c, (const float*)p, (const float*)Ap, n, PAP);
     else launch_dot(c, (const double*)p, (const double*)Ap, n, PAP);
     klaunch(k_pcg_upd_check<T>, red_grid(n), kRedThreads, 0, c.stream, x, r, p, Ap, n, c.scal, RZ, RZN, PAP, IRR,
-            c.partial, c.counter, h, ctl, f32 ? 1 : 0);
+            c.partial, c.counter, h, ctl, f32 ? 1 : 0, mixed ? r32 : (float*)nullptr, YY);
     DP_LAUNCH_CHECK();
   });
 }
@@ -596,10 +618,11 @@ static void ensure_ctl(Ctx& c) {
 
 // The graph-only vector kernels of one inner iteration (FP64 Krylov, FP32
 // multigrid) launched once each outside a graph, without loop control: the
-// scaled FP32 residual, z = ||r|| z32 with r.z, the direction update and the
-// fused x/r update with ||r||^2.  Profilers cannot look inside conditional
-// graph nodes; this is what they time instead.  Vector contents are zeroed
-// and the scalars set to 1, so every value stays finite.
+// scaled FP32 residual (before the loop), r.z from z32, the direction update
+// from z32 and the fused x/r update with ||r||^2 and the next FP32 residual.
+// Profilers cannot look inside conditional graph nodes; this is what they time
+// instead.  Vector contents are zeroed and the scalars set to 1, so every value
+// stays finite.
 void profile_inner_vector_kernels(Ctx& c) {
   ensure_ctl(c);
   const int64_t n = 2 * c.fine.nnod;
@@ -619,13 +642,13 @@ void profile_inner_vector_kernels(Ctx& c) {
   DP_CUDA(cudaMemcpyAsync(c.scal + G_RZ, c.h_scal + 48, 4 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
   DP_CUDA(cudaStreamSynchronize(c.stream));
   klaunch(k_r_to_f32, g_nb(n), 256, 0, c.stream, (const double*)r, r32, c.scal, (int)G_IRR, n);
-  klaunch(k_z_from_f32_dot, red_grid(n), kRedThreads, 0, c.stream, (const float*)z32, z, (const double*)r, c.scal,
-          (int)G_IRR, (int)G_RZN, n, c.partial, c.counter);
-  klaunch(k_pcg_dir_g<double>, g_nb(n), 256, 0, c.stream, p, (const double*)z, Ap, n, (const double*)c.scal,
+  klaunch(k_rz_f32, red_grid(n), kRedThreads, 0, c.stream, (const float*)z32, (const double*)r, c.scal, (int)G_IRR,
+          (int)G_RZN, n, c.partial, c.counter);
+  klaunch(k_pcg_dir_f32z, g_nb(n), 256, 0, c.stream, p, (const float*)z32, Ap, n, (const double*)c.scal, (int)G_IRR,
           (int)G_RZN, (int)G_RZ, (const int*)&ctl->in_it);
   klaunch(k_pcg_upd_check<double>, red_grid(n), kRedThreads, 0, c.stream, x, r, (const double*)p,
           (const double*)Ap, n, c.scal, (int)G_RZ, (int)G_RZN, (int)G_PAP, (int)G_IRR, c.partial, c.counter,
-          (cudaGraphConditionalHandle)0, (DevCtl*)nullptr, 0);
+          (cudaGraphConditionalHandle)0, (DevCtl*)nullptr, 0, r32, (int)G_IRR);
   DP_LAUNCH_CHECK();
 }
 
