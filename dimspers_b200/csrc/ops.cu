@@ -157,30 +157,41 @@ __host__ __device__ constexpr int loc_b(int t, int k) {
 // then local node k = 0..5), so the result is the same bit for bit in every
 // run.  E[(NC k + c) nel + e] holds element e's value c at its local node k.
 // MODE 0: y[NC n + c] += s; 1: y -= s; 2: y = s.
-template <typename T, int NC, int MODE>
-__global__ void __launch_bounds__(256) k_node_gather(const T* __restrict__ E, T* __restrict__ y, int ncr, int nct,
-                                                     int64_t nel) {
-  grid_dep_wait();
-  const int A = 2 * ncr + 1, B = 2 * nct;
-  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (n >= (int64_t)A * B) return;
-  const int b = (int)(n / A), a = (int)(n - (int64_t)b * A);
-  T s[NC];
+// One thread owns the 2x2 node block a = 2i + pa, b = 2j + pb (i <= ncr,
+// j < nct): for each parity class (pa, pb) the elements holding the node are
+// fixed at compile time (local node k of type t holds it iff loc_a(t, k) has
+// the parity of a and loc_b(t, k) that of b; the element's cell is then
+// (i + (pa - loc_a) / 2, j + (pb - loc_b) / 2), theta periodic), so a warp
+// never diverges on them, and neighbouring lanes write neighbouring nodes.
+template <int PA, int PB, typename T, int NC>
+__device__ __forceinline__ void gather_class(const T* __restrict__ E, int i, int j, int ncr, int nct, int64_t nel,
+                                             T s[NC]) {
 #pragma unroll
   for (int c = 0; c < NC; ++c) s[c] = (T)0;
 #pragma unroll
   for (int t = 0; t < 2; ++t) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      const int da = a - loc_a(t, k);
-      int db = b - loc_b(t, k);
-      if (da < 0 || (da & 1) || (da >> 1) >= ncr || (db & 1)) continue;
-      if (db < 0) db += B;
-      const int64_t e = 2 * ((int64_t)(da >> 1) + (int64_t)ncr * (db >> 1)) + t;
+      if ((loc_a(t, k) & 1) != PA || (loc_b(t, k) & 1) != PB) continue;   // resolved at compile time
+      const int ir = i + ((PA - loc_a(t, k)) >> 1);
+      int it = j + ((PB - loc_b(t, k)) >> 1);
+      if (ir < 0 || ir >= ncr) continue;
+      if (it < 0) it += nct;
+      const int64_t e = 2 * ((int64_t)ir + (int64_t)ncr * it) + t;
 #pragma unroll
       for (int c = 0; c < NC; ++c) s[c] += E[(int64_t)(NC * k + c) * nel + e];
     }
   }
+}
+
+template <int PA, int PB, typename T, int NC, int MODE>
+__device__ __forceinline__ void gather_node(const T* __restrict__ E, T* __restrict__ y, int i, int j, int ncr, int nct,
+                                            int64_t nel) {
+  const int a = 2 * i + PA;
+  if (a > 2 * ncr) return;
+  T s[NC];
+  gather_class<PA, PB, T, NC>(E, i, j, ncr, nct, nel, s);
+  const int64_t n = a + (int64_t)(2 * ncr + 1) * (2 * j + PB);
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     T* p = y + NC * n + c;
@@ -190,9 +201,22 @@ __global__ void __launch_bounds__(256) k_node_gather(const T* __restrict__ E, T*
   }
 }
 
+template <typename T, int NC, int MODE>
+__global__ void __launch_bounds__(256) k_node_gather(const T* __restrict__ E, T* __restrict__ y, int ncr, int nct,
+                                                     int64_t nel) {
+  grid_dep_wait();
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= (int64_t)(ncr + 1) * nct) return;
+  const int j = (int)(q / (ncr + 1)), i = (int)(q - (int64_t)j * (ncr + 1));
+  gather_node<0, 0, T, NC, MODE>(E, y, i, j, ncr, nct, nel);
+  gather_node<1, 0, T, NC, MODE>(E, y, i, j, ncr, nct, nel);
+  gather_node<0, 1, T, NC, MODE>(E, y, i, j, ncr, nct, nel);
+  gather_node<1, 1, T, NC, MODE>(E, y, i, j, ncr, nct, nel);
+}
+
 template <typename T>
 void launch_node_gather(const Level& L, const T* E, T* y, int nc, int mode, cudaStream_t s) {
-  const int grid = (int)div_up(L.nnod, 256);
+  const int grid = (int)div_up((int64_t)(L.ncr + 1) * L.nct, 256);
 #define DP_GATHER(NC, M) \
   klaunch(k_node_gather<T, NC, M>, grid, 256, 0, s, E, y, L.ncr, L.nct, (int64_t)L.nel)
   if (nc == 2) {

@@ -23,19 +23,40 @@ def element_nodes(e, ncr, nct):
 
 
 def gather_candidates(n, ncr, nct):
-    """(element, local node) pairs of lattice node n, in the kernel's order."""
-    A, B = 2 * ncr + 1, 2 * nct
+    """(element, local node) pairs of lattice node n, in the kernel's order:
+    node (a, b) = (2 i + pa, 2 j + pb); local node k of type t holds it iff
+    LOC_A[t][k] has the parity pa and LOC_B[t][k] the parity pb, in cell
+    (i + (pa - LOC_A) / 2, j + (pb - LOC_B) / 2), theta periodic."""
+    A = 2 * ncr + 1
     b, a = divmod(n, A)
+    i, pa = divmod(a, 2)
+    j, pb = divmod(b, 2)
     out = []
     for t in (0, 1):
         for k in range(6):
-            da, db = a - LOC_A[t][k], b - LOC_B[t][k]
-            if da < 0 or da & 1 or (da >> 1) >= ncr or db & 1:
+            if LOC_A[t][k] % 2 != pa or LOC_B[t][k] % 2 != pb:
                 continue
-            if db < 0:
-                db += B
-            out.append((2 * ((da >> 1) + ncr * (db >> 1)) + t, k))
+            ir = i + ((pa - LOC_A[t][k]) >> 1)
+            it = j + ((pb - LOC_B[t][k]) >> 1)
+            if ir < 0 or ir >= ncr:
+                continue
+            if it < 0:
+                it += nct
+            out.append((2 * (ir + ncr * it) + t, k))
     return out
+
+
+def thread_blocks(ncr, nct):
+    """Nodes owned by the kernel's threads (2 x 2 blocks, i <= ncr, j < nct)."""
+    A = 2 * ncr + 1
+    owned = []
+    for q in range((ncr + 1) * nct):
+        j, i = divmod(q, ncr + 1)
+        for pb in (0, 1):
+            for pa in (0, 1):
+                if 2 * i + pa <= 2 * ncr:
+                    owned.append(2 * i + pa + A * (2 * j + pb))
+    return owned
 
 
 @pytest.mark.parametrize("ncr,nct", [(1, 2), (1, 4), (2, 4), (3, 6), (4, 32), (5, 10)])
@@ -49,6 +70,8 @@ def test_gather_is_the_inverse_of_the_element_rule(ncr, nct):
         got = gather_candidates(n, ncr, nct)
         assert sorted(got) == sorted(scatter[n]), (n, got, scatter[n])
         assert len(set(got)) == len(got)
+    owned = thread_blocks(ncr, nct)
+    assert sorted(owned) == list(range(nnod))      # every node written by exactly one thread
 
 
 def test_gather_matches_the_reference_connectivity():
