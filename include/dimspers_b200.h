@@ -212,7 +212,9 @@ int dp_assemble(dp_ctx* ctx, int32_t precision);
  * the same U, P and iteration counts bit for bit.  Costs 144 bytes of device
  * scratch per element and two passes per apply.  Needs discontinuous
  * pressure and matrix_free = 0.  Switching it on discards the current assembly
- * (call dp_assemble again); on = 0 returns to the atomic scatter.  (The
+ * (call dp_assemble again); on = 0 returns to the atomic scatter.  A dp_batch
+ * created from this context before a switch keeps the launches it captured:
+ * create the batch again after switching.  (The
  * reference's threaded assembly gets race freedom from element colouring,
  * coloring.jl:1-64; the atomic device scatter has none of its ordering.) */
 int dp_set_deterministic(dp_ctx* ctx, int32_t on);
